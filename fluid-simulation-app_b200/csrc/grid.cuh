@@ -1,0 +1,66 @@
+// grid.cuh — the neighbour grid: cell keys, look-back scan, stable sort.
+#pragma once
+
+#include "common.cuh"
+
+namespace fcu {
+
+struct GridGeom {
+    float min[3];
+    float cell;
+    uint32_t dims[3];
+};
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;  // 4096 u32 per tile
+
+constexpr int kRadixBits = 8;
+constexpr uint32_t kRadix = 1u << kRadixBits;
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortItems = 16;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+
+inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+// Digit passes for keys below `cells`.
+inline int radix_passes(uint32_t cells) {
+    uint32_t maxkey = cells > 0 ? cells - 1 : 0;
+    int bits = 0;
+    while (maxkey) {
+        bits++;
+        maxkey >>= 1;
+    }
+    int p = (bits + kRadixBits - 1) / kRadixBits;
+    return p < 1 ? 1 : p;
+}
+
+// Scratch of one grid build, carved from one device allocation.
+struct GridWork {
+    uint32_t *counts;              // [cells], zero between builds
+    unsigned long long *scan_ctl;  // (1 + passes) look-back regions, zeroed per build
+    size_t scan_ctl_bytes;
+    uint32_t *hist;                // [kRadix * tiles]
+    uint32_t *k1, *k2, *v1, *v2;   // ping-pong keys / values
+    uint32_t *err;                 // device error word (may alias the sim's)
+    int passes;
+    uint32_t cells, n;
+};
+
+size_t grid_work_bytes(uint32_t n, uint32_t cells);
+// Carves `ws` (at least grid_work_bytes) into a GridWork.
+GridWork grid_work_carve(void *ws, uint32_t n, uint32_t cells, uint32_t *err);
+
+// Enqueues count -> scan -> stable sort on `stream`. `keys` receives each
+// input's cell key, `starts` the exclusive scan with starts[cells] = n,
+// `perm` the stable permutation. When `counts_zeroed` is false the counts
+// are cleared first. `ring`/`cur`/`solve` (may be null) let the key kernel
+// also fetch the substep's Step block from the ring.
+cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t n,
+                               const GridGeom &g, uint32_t *keys, uint32_t *starts,
+                               uint32_t *perm, GridWork &w, bool counts_zeroed,
+                               const DevStep *ring, DevStep *cur, DevSolve *solve,
+                               uint32_t ring_size);
+
+}  // namespace fcu

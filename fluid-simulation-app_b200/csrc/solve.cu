@@ -1,0 +1,820 @@
+// solve.cu — DFSPH sweeps for sm_100a, one thread per particle.
+//
+// Reference: crates/fluid-core/src/sim_solve.wgsl (whole file). The reference
+// splits each particle over 8 subgroup lanes; here a particle is one thread
+// (a million particles fill 148 SMs many times over) and its neighbours are
+// summed in one fixed order: the 27 stencil cells with x fastest, walked as
+// nine rows of three x-adjacent cells, which are one contiguous slot range of
+// the cell-ordered working set; slots ascending. Neighbour lists hold the slot
+// j only (4 bytes, slot-major so a warp's k-th entries are adjacent); the
+// kernel gradient is recomputed from the positions, which do not move inside
+// a substep, bit for bit the value density_div found.
+//
+// Compiled with -fmad=false: no product-sum is fused unless written so.
+#include <cuda_fp16.h>
+
+#include "solve.cuh"
+
+namespace fcu {
+
+namespace {
+
+// sim_solve.wgsl:84-172
+constexpr float TOUCH_RATE = 40.0f;
+constexpr float K_NEAR = 3000.0f;
+constexpr float DYNAMIC_VISCOSITY = 1.002e-3f;
+constexpr float HEAT_CAPACITY = 4184.0f;
+constexpr float CONDUCTIVITY = 0.598f;
+constexpr float EXPANSION = 2.07e-4f;
+constexpr float SIGMA_WATER = 0.0728f;
+constexpr float LATTICE_SIGMA = 0.8665f;
+constexpr float COS_CONTACT = -0.342f;
+constexpr float HUGE_F = 1e30f;  // sim_solve.wgsl:792
+
+__device__ __forceinline__ float kernel_q(const DevParams &P, float q) {  // :176-182
+    if (q < 1.0f) return P.sigma * (1.0f - 1.5f * q * q * (1.0f - 0.5f * q));
+    const float t = 2.0f - q;
+    return P.sigma * 0.25f * t * t * t;
+}
+
+__device__ __forceinline__ F3 grad_q(const DevParams &P, F3 x, float r, float q) {  // :184-196
+    if (r < 1e-9f) return f3(0.f, 0.f, 0.f);
+    float dw;
+    if (q < 1.0f) {
+        dw = P.sigma_h * (-3.0f * q + 2.25f * q * q);
+    } else {
+        const float t = 2.0f - q;
+        dw = P.sigma_h * (-0.75f * t * t);
+    }
+    return (dw / r) * x;
+}
+
+__device__ __forceinline__ float cohesion(float r, float c, float k, float near) {  // :201-210
+    if (r >= c || r < 1e-9f) return 0.0f;
+    const float a = (c - r) * (c - r) * (c - r) * r * r * r;
+    if (2.0f * r > c) return k * a;
+    return k * (2.0f * a - near);
+}
+
+__device__ __forceinline__ float wall_density(float t) {  // :213-222
+    if (t >= 2.0f) return 0.0f;
+    const float t3 = t * t * t;
+    if (t < 1.0f) return 0.5f - 0.7f * t + t3 * (1.0f / 3.0f + t * t * (-0.15f + 0.05f * t));
+    return 8.0f / 15.0f - 0.8f * t + t3 * (2.0f / 3.0f + t * (-0.5f + t * (0.15f - t / 60.0f)));
+}
+
+__device__ __forceinline__ float wall_gradient(float t) {  // :226-235
+    if (t >= 2.0f) return 0.0f;
+    const float t2 = t * t;
+    if (t < 1.0f) return 0.7f + t2 * (-1.0f + t2 * (0.75f - t * 0.3f));
+    return 0.8f + t2 * (-2.0f + t * (2.0f + t * (-0.75f + t * 0.1f)));
+}
+
+__device__ __forceinline__ float wedge(float t1, float t2) {  // :249-270
+    if (t1 * t1 + t2 * t2 >= 4.0f) return 0.0f;
+    return (2.5005807e-01f +
+            t2 * (-3.4681153e-01f +
+                  t2 * (-4.0986882e-02f +
+                        t2 * (3.0301620e-01f +
+                              t2 * (-1.9202736e-01f + t2 * (4.6947582e-02f + t2 * (-3.8543515e-03f))))))) +
+           t1 * ((-3.4681153e-01f +
+                  t2 * (4.8587248e-01f +
+                        t2 * (1.0092180e-02f +
+                              t2 * (-2.9978363e-01f + t2 * (1.5320335e-01f + t2 * (-2.2544282e-02f)))))) +
+                 t1 * ((-4.0986882e-02f +
+                        t2 * (1.0092180e-02f +
+                              t2 * (-5.4145610e-02f + t2 * (7.9597369e-02f + t2 * (-2.3350373e-02f))))) +
+                       t1 * ((3.0301620e-01f +
+                              t2 * (-2.9978363e-01f + t2 * (7.9597369e-02f + t2 * (-8.2431946e-03f)))) +
+                             t1 * ((-1.9202736e-01f + t2 * (1.5320335e-01f + t2 * (-2.3350373e-02f))) +
+                                   t1 * ((4.6947582e-02f + t2 * (-2.2544282e-02f)) +
+                                         t1 * (-3.8543515e-03f))))));
+}
+
+__device__ __forceinline__ float wedge_d(float t1, float t2) {  // :272-293
+    if (t1 * t1 + t2 * t2 >= 4.0f) return 0.0f;
+    return (-3.4611994e-01f +
+            t2 * (4.4757673e-01f +
+                  t2 * (1.1932939e-01f +
+                        t2 * (-4.6460101e-01f +
+                              t2 * (2.7637253e-01f + t2 * (-6.2846025e-02f + t2 * (4.3871652e-03f))))))) +
+           t1 * ((-6.3622823e-02f +
+                  t2 * (2.0521006e-01f +
+                        t2 * (-3.7311339e-01f +
+                              t2 * (3.7508155e-01f + t2 * (-1.6629713e-01f + t2 * (2.5030129e-02f)))))) +
+                 t1 * ((7.8352497e-01f +
+                        t2 * (-1.2658344e+00f +
+                              t2 * (5.8898945e-01f + t2 * (-1.0772903e-01f + t2 * (1.3535777e-02f))))) +
+                       t1 * ((-4.9470084e-01f +
+                              t2 * (9.1302071e-01f + t2 * (-3.4330355e-01f + t2 * (2.4034609e-02f)))) +
+                             t1 * ((-2.5605481e-02f + t2 * (-2.0067981e-01f + t2 * (5.9854468e-02f))) +
+                                   t1 * ((8.8898623e-02f + t2 * (3.9914838e-03f)) +
+                                         t1 * (-1.7788321e-02f))))));
+}
+
+__device__ __forceinline__ float wall_adhesion(float t) {  // :334-340
+    const float u = clampf(2.0f - t, 0.0f, 2.0f);
+    return u * u *
+           (1.7847015e-3f +
+            u * (3.3392196e-3f + u * (-4.3394677e-3f + u * (1.6711868e-3f + u * (-2.1788750e-4f)))));
+}
+
+__device__ __forceinline__ float wedge_dsum(float t, float a, float b, float c, float d) {  // :295
+    return wedge_d(t, a) + wedge_d(t, b) + wedge_d(t, c) + wedge_d(t, d);
+}
+
+__device__ __forceinline__ float wedge_sum(F3 tl, F3 th) {  // :299-304
+    float w = wedge(tl.x, tl.y) + wedge(tl.x, th.y) + wedge(th.x, tl.y) + wedge(th.x, th.y);
+    w += wedge(tl.x, tl.z) + wedge(tl.x, th.z) + wedge(th.x, tl.z) + wedge(th.x, th.z);
+    w += wedge(tl.y, tl.z) + wedge(tl.y, th.z) + wedge(th.y, tl.z) + wedge(th.y, th.z);
+    return w;
+}
+
+__device__ __forceinline__ F3 wall_lo(const DevParams &P) { return f3(P.wall_lo[0], P.wall_lo[1], P.wall_lo[2]); }
+__device__ __forceinline__ F3 wall_hi(const DevParams &P) { return f3(P.wall_hi[0], P.wall_hi[1], P.wall_hi[2]); }
+
+__device__ F3 wall_grad_sum(const DevParams &P, F3 pos) {  // :310-328
+    const F3 lo = wall_lo(P), hi = wall_hi(P);
+    const float inv_h = 1.0f / P.h;
+    const F3 tl = (pos - lo) * inv_h;
+    const F3 th = (hi - pos) * inv_h;
+    const float scale = P.rho0 * inv_h;
+    F3 g = f3(0.f, 0.f, 0.f);
+    g.x -= scale * (wall_gradient(tl.x) + wedge_dsum(tl.x, tl.y, th.y, tl.z, th.z));
+    g.x += scale * (wall_gradient(th.x) + wedge_dsum(th.x, tl.y, th.y, tl.z, th.z));
+    g.y -= scale * (wall_gradient(tl.y) + wedge_dsum(tl.y, tl.x, th.x, tl.z, th.z));
+    g.y += scale * (wall_gradient(th.y) + wedge_dsum(th.y, tl.x, th.x, tl.z, th.z));
+    g.z -= scale * (wall_gradient(tl.z) + wedge_dsum(tl.z, tl.x, th.x, tl.y, th.y));
+    g.z += scale * (wall_gradient(th.z) + wedge_dsum(th.z, tl.x, th.x, tl.y, th.y));
+    return g;
+}
+
+__device__ F3 wall_adh_sum(const DevParams &P, F3 pos) {  // :349-361
+    const F3 lo = wall_lo(P), hi = wall_hi(P);
+    const float inv_h = 1.0f / P.h;
+    F3 a = f3(0.f, 0.f, 0.f);
+    a.x -= wall_adhesion((pos.x - lo.x) * inv_h);
+    a.x += wall_adhesion((hi.x - pos.x) * inv_h);
+    a.y -= wall_adhesion((pos.y - lo.y) * inv_h);
+    a.y += wall_adhesion((hi.y - pos.y) * inv_h);
+    a.z -= wall_adhesion((pos.z - lo.z) * inv_h);
+    a.z += wall_adhesion((hi.z - pos.z) * inv_h);
+    return a;
+}
+
+// exp for per-particle arguments: Cody-Waite reduction by ln2 (16-bit head,
+// tail), degree-7 Taylor polynomial of e^r in Horner form, scale by 2^k
+// through the exponent bits. The CPU oracle evaluates the same sequence.
+__device__ __forceinline__ float det_exp(float x) {
+    if (!(x > -87.0f)) return 0.0f;
+    if (x > 88.0f) x = 88.0f;
+    const float kf = rintf(x * 1.44269504f);
+    float r = x - kf * 0.693145752f;
+    r = r - kf * 1.42860677e-6f;
+    float p = 1.98412698e-4f;
+    p = p * r + 1.38888889e-3f;
+    p = p * r + 8.33333333e-3f;
+    p = p * r + 4.16666667e-2f;
+    p = p * r + 1.66666667e-1f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    const int k = (int)kf;
+    return p * __uint_as_float((uint32_t)(k + 127) << 23);
+}
+
+// The neighbour's kernel gradient from the two positions (grad_q of
+// density_div's pair, recomputed).
+__device__ __forceinline__ F3 pair_grad(const DevParams &P, F3 pos, float4 pj) {
+    const F3 x = pos - xyz(pj);
+    const float r2 = dot(x, x);
+    const float r = sqrtf(r2);
+    const float q = r * P.inv_h;
+    return grad_q(P, x, r, q);
+}
+
+// ---- gather into the working set (sim_grid.wgsl:52-63) -------------------
+__global__ void __launch_bounds__(256) k_gather(SimBufs b, uint32_t n) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint32_t i = __ldg(&b.perm[k]);
+    if (i >= n) i = k;  // only after a grid build that gave up; keeps reads in bounds
+    b.wpos[k] = __ldg(&b.pos[i]);
+    b.wvel[k] = __ldg(&b.vel[i]);
+    b.wpvel[k] = __ldg(&b.pvel[i]);
+    b.wpp[k] = __ldg(&b.pp[i]);
+    b.wtemp[k] = __ldg(&b.temp[i]);
+    b.wid[k] = __ldg(&b.id[i]);
+}
+
+// ---- density_div (sim_solve.wgsl:411-518) --------------------------------
+__global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimBufs b,
+                                                               const DevStep *__restrict__ st,
+                                                               DevSolve *solve,
+                                                               unsigned long long *acc) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = st->s.dt;
+    unsigned long long term = 0;
+    if (i < n) {
+        const float4 *__restrict__ wpos = b.wpos;
+        const float4 *__restrict__ wvel = b.wvel;
+        const F3 pos = xyz(__ldg(&wpos[i]));
+        const F3 vel = xyz(__ldg(&wvel[i]));
+        const int bx = (int)axis_cell(pos.x, P.box_min[0], P.cell, P.dims[0]);
+        const int by = (int)axis_cell(pos.y, P.box_min[1], P.cell, P.dims[1]);
+        const int bz = (int)axis_cell(pos.z, P.box_min[2], P.cell, P.dims[2]);
+        const int dx = (int)P.dims[0], dy = (int)P.dims[1], dz = (int)P.dims[2];
+        const int cx0 = bx > 0 ? bx - 1 : 0;
+        const int cx1 = bx + 1 < dx ? bx + 1 : dx - 1;
+        float w_sum = P.sigma;
+        float rho_near = 0.0f;
+        F3 grad_sum = f3(0.f, 0.f, 0.f);
+        float grad_sq = 0.0f;
+        float drho = 0.0f;
+        uint32_t found = 0;
+        const uint32_t cap = P.nbr_cap;
+        for (int oz = -1; oz <= 1; ++oz) {
+            const int cz = bz + oz;
+            if (cz < 0 || cz >= dz) continue;
+            for (int oy = -1; oy <= 1; ++oy) {
+                const int cy = by + oy;
+                if (cy < 0 || cy >= dy) continue;
+                const uint32_t row = ((uint32_t)cz * (uint32_t)dy + (uint32_t)cy) * (uint32_t)dx;
+                const uint32_t s = __ldg(&b.starts[row + cx0]);
+                uint32_t e = __ldg(&b.starts[row + cx1 + 1]);
+                if (e > n) e = n;  // starts never exceed n unless a scan gave up
+                for (uint32_t k = s; k < e; ++k) {
+                    if (k == i) continue;
+                    const F3 x = pos - xyz(__ldg(&wpos[k]));
+                    const float r2 = dot(x, x);
+                    if (r2 >= P.support_sq) continue;
+                    const float r = sqrtf(r2);
+                    const float q = r * P.inv_h;
+                    w_sum += kernel_q(P, q);
+                    const float wn = fmaxf(1.0f - q, 0.0f);
+                    rho_near += wn * wn * wn;
+                    const F3 gw = grad_q(P, x, r, q);
+                    grad_sum = grad_sum + gw;
+                    grad_sq += dot(gw, gw);
+                    drho += dot(vel - xyz(__ldg(&wvel[k])), gw);
+                    if (found < cap) b.nbr[(size_t)found * n + i] = k;
+                    found++;
+                }
+            }
+        }
+        b.nbr_n[i] = found < cap ? found : cap;
+        if (found > cap) atomicAdd(&solve->nbr_over, found - cap);
+        float rho = P.mass * w_sum;
+        grad_sq = P.mass * P.mass * grad_sq;
+        drho = P.mass * drho;
+        grad_sum = P.mass * grad_sum;
+        const F3 lo = wall_lo(P), hi = wall_hi(P);
+        const F3 tl = (pos - lo) * P.inv_h;
+        const F3 th = (hi - pos) * P.inv_h;
+        float fill = 0.0f;
+        fill += wall_density(tl.x) + wall_density(th.x);
+        fill += wall_density(tl.y) + wall_density(th.y);
+        fill += wall_density(tl.z) + wall_density(th.z);
+        fill -= wedge_sum(tl, th);
+        rho += P.rho0 * fill;
+        const F3 wg = wall_grad_sum(P, pos);
+        b.wgrad[i] = make_float4(wg.x, wg.y, wg.z, 0.0f);
+        grad_sum = grad_sum + wg;
+        b.density[i] = rho;
+        b.rho_near[i] = rho_near;
+        const float a = rho / fmaxf(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
+        b.alpha[i] = a;
+        drho += dot(vel, wg);
+        b.kd[i] = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
+        term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
+    }
+    accumulate_fixed(acc, term);
+}
+
+// ---- divergence predictor for a later divergence iteration ---------------
+__global__ void __launch_bounds__(kSolveThreads) k_div_kappa(DevParams P, SimBufs b,
+                                                             const DevStep *__restrict__ st,
+                                                             unsigned long long *acc) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = st->s.dt;
+    unsigned long long term = 0;
+    if (i < n) {
+        const F3 pos = xyz(__ldg(&b.wpos[i]));
+        const F3 vel = xyz(__ldg(&b.wvel[i]));
+        const uint32_t cnt = __ldg(&b.nbr_n[i]);
+        float drho = 0.0f;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
+            const F3 e = pair_grad(P, pos, __ldg(&b.wpos[j]));
+            drho += dot(vel - xyz(__ldg(&b.wvel[j])), e);
+        }
+        drho = P.mass * drho;
+        drho += dot(vel, xyz(__ldg(&b.wgrad[i])));
+        const float rho = __ldg(&b.density[i]);
+        b.kd[i] = fmaxf(drho, 0.0f) * __ldg(&b.alpha[i]) / fmaxf(dt, 1e-9f) / rho;
+        term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
+    }
+    accumulate_fixed(acc, term);
+}
+
+// kappa_partial (sim_solve.wgsl:596-606), sequential over the list.
+__device__ __forceinline__ F3 kappa_sum(const DevParams &P, const SimBufs &b, uint32_t i,
+                                        uint32_t n, F3 pos, float kd_i) {
+    const uint32_t cnt = __ldg(&b.nbr_n[i]);
+    F3 dv = f3(0.f, 0.f, 0.f);
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
+        const F3 e = pair_grad(P, pos, __ldg(&b.wpos[j]));
+        dv = dv + (kd_i + __ldg(&b.kd[j])) * e;
+    }
+    return dv;
+}
+
+// ---- apply_kappa_wide: div_apply / den_apply (sim_solve.wgsl:608-621) -----
+// For the density iterations the applied pressure k*rho that den_kappa held
+// back joins the pressure here, with the kappa it belongs to.
+__global__ void __launch_bounds__(kSolveThreads) k_apply(DevParams P, SimBufs b,
+                                                         const DevStep *__restrict__ st,
+                                                         int add_pressure) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float dt = st->s.dt;
+    const F3 pos = xyz(__ldg(&b.wpos[i]));
+    const float kd_i = b.kd[i];
+    const F3 total = kappa_sum(P, b, i, n, pos, kd_i);
+    const F3 dv_full = P.mass * total + kd_i * xyz(__ldg(&b.wgrad[i]));
+    const float4 was = b.wvel[i];
+    const F3 v = xyz(was) - dt * dv_full;
+    b.wvel[i] = make_float4(v.x, v.y, v.z, was.w);
+    if (add_pressure) b.pressure[i] += b.pinc[i];
+}
+
+// ---- forces_eval (sim_solve.wgsl:524-592) ---------------------------------
+__global__ void __launch_bounds__(kSolveThreads) k_forces_eval(DevParams P, SimBufs b) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float coh_c = 2.0f * P.h;
+    const float c3 = coh_c * coh_c * coh_c;
+    const float coh_k = 32.0f / (3.14159265f * c3 * c3 * c3);
+    const float coh_near = c3 * c3 / 64.0f;
+    const float c = 2.0f * P.h;
+    const float gamma = SIGMA_WATER * 7040.0f / (21.0f * LATTICE_SIGMA * P.rho0 * P.rho0 * c * c);
+    const float beta =
+        SIGMA_WATER * (1.0f + COS_CONTACT) * 1558.4f / (LATTICE_SIGMA * P.rho0 * P.rho0 * c * c);
+    const float visc_k = 2.0f * DYNAMIC_VISCOSITY;
+    const float heat_k = 2.0f * CONDUCTIVITY / HEAT_CAPACITY;
+    const float diss_k = 0.5f * DYNAMIC_VISCOSITY / HEAT_CAPACITY;
+
+    const F3 pos = xyz(__ldg(&b.wpos[i]));
+    const float near_i = __ldg(&b.rho_near[i]);
+    const F3 vel = xyz(__ldg(&b.wvel[i]));
+    const float temp = __ldg(&b.wtemp[i]);
+    const float rho_i = __ldg(&b.density[i]);
+    const uint32_t cnt = __ldg(&b.nbr_n[i]);
+    F3 visc = f3(0.f, 0.f, 0.f), blend = f3(0.f, 0.f, 0.f), near = f3(0.f, 0.f, 0.f),
+       tension = f3(0.f, 0.f, 0.f);
+    float heat = 0.0f;
+    for (uint32_t k = 0; k < cnt; ++k) {
+        const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
+        const float4 pj = __ldg(&b.wpos[j]);
+        const F3 e = pair_grad(P, pos, pj);
+        const F3 x = pos - xyz(pj);
+        const float r2 = dot(x, x);
+        const float r = sqrtf(r2);
+        const float rho_j = __ldg(&b.density[j]);
+        const float f = dot(x, e) / (r2 + 0.01f * P.h * P.h);
+        const float pair = P.mass / (rho_i * rho_j) * f;
+        const F3 dv = vel - xyz(__ldg(&b.wvel[j]));
+        const float wn = fmaxf(1.0f - r * P.inv_h, 0.0f);
+        near = near + ((near_i + __ldg(&b.rho_near[j])) * wn * wn) * (x / fmaxf(r, 1e-5f));
+        visc = visc + (visc_k * pair) * dv;
+        blend = blend - (P.mass / rho_j * kernel_q(P, r * P.inv_h)) * dv;
+        heat += heat_k * pair * (temp - __ldg(&b.wtemp[j]));
+        heat -= diss_k * pair * dot(dv, dv);
+        const float corr = 2.0f * P.rho0 / (rho_i + rho_j);
+        tension = tension - ((corr * P.mass * cohesion(r, coh_c, coh_k, coh_near)) * x) / fmaxf(r, 1e-9f);
+    }
+    const F3 adh = (beta * P.rho0) * wall_adh_sum(P, pos);
+    const F3 acc = visc + K_NEAR * near + gamma * tension + adh;
+    b.accel[i] = make_float4(acc.x, acc.y, acc.z, heat);
+    b.xsph[i] = make_float4(blend.x, blend.y, blend.z, 0.0f);
+    const float half = 0.5f * __ldg(&b.wpp[i]);
+    b.kd[i] = half / (rho_i * rho_i);
+    b.pressure[i] = half;
+}
+
+// fingers (sim_solve.wgsl:103-127)
+__device__ __forceinline__ F3 fingers(const FluidStep &st, F3 pos, F3 v) {
+    float px = 0.0f, py = 0.0f, weight = 0.0f;
+    const uint32_t tn = st.touch_n < 5u ? st.touch_n : 5u;
+    for (uint32_t t = 0; t < tn; ++t) {
+        const float *tc = st.touches[t];
+        const float dx = pos.x - tc[0], dy = pos.y - tc[1];
+        const float q2 = (dx * dx + dy * dy) / (st.touch_r * st.touch_r);
+        if (q2 < 1.0f) {
+            const float w = (1.0f - q2) * (1.0f - q2);
+            px += w * tc[2];
+            py += w * tc[3];
+            weight += w;
+        }
+    }
+    if (weight <= 0.0f) return v;
+    const float a = 1.0f - det_exp(-TOUCH_RATE * weight * st.dt);
+    return f3(mixf(v.x, px / weight, a), mixf(v.y, py / weight, a), v.z);
+}
+
+// ---- forces_den_apply (sim_solve.wgsl:630-663) -----------------------------
+__global__ void __launch_bounds__(kSolveThreads) k_forces_apply(DevParams P, SimBufs b,
+                                                                const DevStep *__restrict__ stp) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const FluidStep &st = stp->s;
+    const float dt = st.dt;
+    const F3 pos = xyz(__ldg(&b.wpos[i]));
+    const float kd_i = b.kd[i];
+    const F3 total = kappa_sum(P, b, i, n, pos, kd_i);
+    const float4 a = __ldg(&b.accel[i]);
+    const F3 r = pos;
+    const float4 was = b.wvel[i];
+    const F3 v = xyz(was);
+    const F3 force = f3(st.force[0], st.force[1], st.force[2]);
+    const F3 omega = f3(st.omega[0], st.omega[1], st.omega[2]);
+    const F3 domega = f3(st.domega[0], st.domega[1], st.domega[2]);
+    const F3 fict = -cross(domega, r) - cross(omega, cross(omega, r)) - 2.0f * cross(omega, v);
+    const F3 forced = fingers(st, r, v + dt * (force + fict + xyz(a)) + stp->xsph_blend * xyz(__ldg(&b.xsph[i])));
+    b.wtemp[i] += dt * a.w;
+    const F3 dv_full = P.mass * total + kd_i * xyz(__ldg(&b.wgrad[i]));
+    const F3 o = forced - dt * dv_full;
+    b.wvel[i] = make_float4(o.x, o.y, o.z, was.w);
+}
+
+// ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
+__global__ void __launch_bounds__(kSolveThreads) k_den_kappa(DevParams P, SimBufs b,
+                                                             const DevStep *__restrict__ st,
+                                                             unsigned long long *acc) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float dt = st->s.dt;
+    unsigned long long term = 0;
+    if (i < n) {
+        const F3 pos = xyz(__ldg(&b.wpos[i]));
+        const F3 vel = xyz(__ldg(&b.wvel[i]));
+        const uint32_t cnt = __ldg(&b.nbr_n[i]);
+        float drho = 0.0f;
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
+            const F3 e = pair_grad(P, pos, __ldg(&b.wpos[j]));
+            drho += dot(vel - xyz(__ldg(&b.wvel[j])), e);
+        }
+        const float rho = __ldg(&b.density[i]);
+        drho = P.mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
+        const float rho_star = rho + dt * drho;
+        const float kk = fmaxf(rho_star - P.rho0, 0.0f) * __ldg(&b.alpha[i]) / (dt * dt);
+        b.kd[i] = kk / rho;
+        b.pinc[i] = kk * rho;
+        term = fixed_term((double)rho_star / (double)P.rho0 - 1.0);
+    }
+    accumulate_fixed(acc, term);
+}
+
+// ---- integrate (sim_solve.wgsl:709-756) ------------------------------------
+// With div_slot >= 0 (the fixed schedule) thread 0 also records the
+// substep's residuals from the accumulator slots of the last divergence and
+// density predictions, and the iteration counts.
+__global__ void __launch_bounds__(256) k_integrate(DevParams P, SimBufs b,
+                                                   const DevStep *__restrict__ stp, DevSolve *solve,
+                                                   int div_slot, int den_slot, int div_iters,
+                                                   int den_iters) {
+    const uint32_t n = P.count;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const FluidStep &st = stp->s;
+    bool clamped_speed = false;
+    if (i < n) {
+        const float4 was = __ldg(&b.wvel[i]);
+        F3 v = xyz(was);
+        const float speed = len(v);
+        const float rho = __ldg(&b.density[i]);
+        const float ceiling = rho < 0.5f * P.rho0 ? 3.0f * st.v_clamp : st.v_clamp;
+        if (speed > ceiling) {
+            v = v * (ceiling / speed);
+            clamped_speed = true;
+        }
+        const float4 pv = __ldg(&b.wpvel[i]);
+        const float accel = len(v - xyz(pv)) / st.dt;
+        const F3 pp = xyz(__ldg(&b.wpos[i])) + v * st.dt;
+        const F3 cl = f3(clampf(pp.x, P.wall_lo[0], P.wall_hi[0]), clampf(pp.y, P.wall_lo[1], P.wall_hi[1]),
+                         clampf(pp.z, P.wall_lo[2], P.wall_hi[2]));
+        if (cl.x != pp.x) v.x = 0.0f;
+        if (cl.y != pp.y) v.y = 0.0f;
+        if (cl.z != pp.z) v.z = 0.0f;
+        const float chase = stp->chase;
+        const float pressure = __ldg(&b.pressure[i]);
+        b.pos[i] = make_float4(cl.x, cl.y, cl.z, 0.0f);
+        b.vel[i] = make_float4(v.x, v.y, v.z, mixf(was.w, accel, chase));
+        b.pvel[i] = make_float4(v.x, v.y, v.z, mixf(pv.w, pressure, chase));
+        const float dp = pressure - __ldg(&b.wpp[i]);
+        b.pp[i] = pressure;
+        const float t = __ldg(&b.wtemp[i]);
+        b.temp[i] = t + t * EXPANSION / (rho * HEAT_CAPACITY) * dp;
+        b.id[i] = __ldg(&b.wid[i]);
+    }
+    const uint32_t m = __ballot_sync(0xffffffffu, clamped_speed);
+    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&solve->clamp_count, __popc(m));
+    if (i == 0) {
+        solve->substeps += 1ull;
+        if (div_slot >= 0) {
+            solve->div_res = (double)solve->acc_div[div_slot] / kFixedScale / (double)n;
+            solve->den_res =
+                den_slot >= 0 ? (double)solve->acc_den[den_slot] / kFixedScale / (double)n : 0.0;
+            solve->div_iters = (uint32_t)div_iters;
+            solve->den_iters = (uint32_t)den_iters;
+        }
+    }
+}
+
+// Records the residual of slot `slot` (fixed schedule) or of slot 0 and
+// clears it (tolerance loop).
+__global__ void k_finish_residual(DevSolve *solve, uint32_t n, int which, int count_iter,
+                                  int reset_iters) {
+    unsigned long long *acc = which == 0 ? solve->acc_div : solve->acc_den;
+    const double res = (double)acc[0] / kFixedScale / (double)n;
+    acc[0] = 0ull;
+    uint32_t *iters = which == 0 ? &solve->div_iters : &solve->den_iters;
+    if (reset_iters) *iters = 0;
+    if (count_iter) *iters += 1;
+    if (which == 0) solve->div_res = res;
+    else solve->den_res = res;
+}
+
+// ---- reduce_stats (sim_solve.wgsl:800-874) ---------------------------------
+// Per-block partials, then one block folds them; min and max are exact in
+// any order and the compression sum is an integer sum.
+__global__ void __launch_bounds__(kStatsThreads) k_stats_partial(DevParams P, SimBufs b) {
+    const uint32_t n = P.count;
+    __shared__ float sh[12][kStatsThreads / 32];
+    __shared__ unsigned long long ssum[kStatsThreads / 32];
+    float m = 0.0f, lo = HUGE_F, hi = -HUGE_F;
+    float v_lo = HUGE_F, v_hi = -HUGE_F, a_lo = HUGE_F, a_hi = -HUGE_F;
+    float p_lo = HUGE_F, p_hi = -HUGE_F, t_lo = HUGE_F, t_hi = -HUGE_F;
+    unsigned long long sum = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float d = __ldg(&b.density[i]);
+        const float c = d / P.rho0 - 1.0f;
+        sum += fixed_term((double)fmaxf(c, 0.0f));
+        m = fmaxf(m, c);
+        lo = fminf(lo, d);
+        hi = fmaxf(hi, d);
+        const float4 q = __ldg(&b.vel[i]);
+        const float speed = len(xyz(q));
+        v_lo = fminf(v_lo, speed);
+        v_hi = fmaxf(v_hi, speed);
+        a_lo = fminf(a_lo, q.w);
+        a_hi = fmaxf(a_hi, q.w);
+        const float pr = __ldg(&b.pvel[i]).w;
+        p_lo = fminf(p_lo, pr);
+        p_hi = fmaxf(p_hi, pr);
+        const float t = __ldg(&b.temp[i]);
+        t_lo = fminf(t_lo, t);
+        t_hi = fmaxf(t_hi, t);
+    }
+    float vals[12] = {m, lo, hi, v_lo, v_hi, a_lo, a_hi, p_lo, p_hi, t_lo, t_hi, 0.0f};
+    const bool is_max[12] = {true, false, true, false, true, false, true, false, true, false, true, true};
+#pragma unroll
+    for (int q = 0; q < 11; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float y = __shfl_xor_sync(0xffffffffu, vals[q], o);
+            vals[q] = is_max[q] ? fmaxf(vals[q], y) : fminf(vals[q], y);
+        }
+    }
+    sum = warp_sum_u64(sum);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+#pragma unroll
+        for (int q = 0; q < 11; ++q) sh[q][warp] = vals[q];
+        ssum[warp] = sum;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float out[11];
+        unsigned long long s = 0;
+        for (int q = 0; q < 11; ++q) out[q] = sh[q][0];
+        for (int w = 0; w < kStatsThreads / 32; ++w) {
+            for (int q = 0; q < 11; ++q) out[q] = is_max[q] ? fmaxf(out[q], sh[q][w]) : fminf(out[q], sh[q][w]);
+            s += ssum[w];
+        }
+        for (int q = 0; q < 11; ++q) b.stats_part[blockIdx.x * 12 + q] = out[q];
+        atomicAdd(b.stats_acc, s);
+    }
+}
+
+__global__ void k_stats_final(DevParams P, SimBufs b, DevSolve *solve, uint32_t blocks) {
+    if (threadIdx.x != 0) return;
+    const bool is_max[11] = {true, false, true, false, true, false, true, false, true, false, true};
+    float out[11];
+    for (int q = 0; q < 11; ++q) out[q] = b.stats_part[q];
+    for (uint32_t k = 1; k < blocks; ++k)
+        for (int q = 0; q < 11; ++q) {
+            const float v = b.stats_part[k * 12 + q];
+            out[q] = is_max[q] ? fmaxf(out[q], v) : fminf(out[q], v);
+        }
+    float *s = b.stats;
+    s[0] = (float)((double)*b.stats_acc / kFixedScale / (double)P.count);
+    *b.stats_acc = 0ull;
+    s[1] = fmaxf(out[0], 0.0f);
+    s[2] = out[1];
+    s[3] = out[2];
+    s[11] = out[3];
+    s[6] = out[4];
+    s[12] = out[5];
+    s[13] = out[6];
+    s[4] = out[7];
+    s[5] = out[8];
+    s[7] = out[9];
+    s[8] = out[10];
+    s[9] = (float)solve->clamp_count;
+    s[10] = (float)solve->nbr_over;
+}
+
+// ---- tracers (sim_tracers.wgsl) ----------------------------------------------
+__device__ __forceinline__ uint32_t pcg(uint32_t x) {  // :54-58
+    uint32_t h = x * 747796405u + 2891336453u;
+    h = ((h >> ((h >> 28u) + 4u)) ^ h) * 277803737u;
+    return (h >> 22u) ^ h;
+}
+
+__device__ __forceinline__ int32_t to_fixed(float v) {  // i32(v * 65536): saturating, toward zero
+    return __float2int_rz(v * 65536.0f);
+}
+
+__global__ void __launch_bounds__(256) k_splat(DevParams P, SimBufs b) {  // :98-114
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.count) return;
+    const float4 p = __ldg(&b.pos[i]);
+    const uint32_t cx = axis_cell(p.x, P.box_min[0], P.cell, P.dims[0]);
+    const uint32_t cy = axis_cell(p.y, P.box_min[1], P.cell, P.dims[1]);
+    const uint32_t cz = axis_cell(p.z, P.box_min[2], P.cell, P.dims[2]);
+    const uint32_t c = ((cz * P.dims[1] + cy) * P.dims[0] + cx) * 4u;
+    const float4 v = __ldg(&b.vel[i]);
+    atomicAdd(&b.vel_grid[c], to_fixed(v.x));
+    atomicAdd(&b.vel_grid[c + 1], to_fixed(v.y));
+    atomicAdd(&b.vel_grid[c + 2], to_fixed(v.z));
+    atomicAdd(&b.vel_grid[c + 3], 1);
+}
+
+__global__ void __launch_bounds__(256) k_resolve(SimBufs b, uint32_t cells) {  // :122-138
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cells) return;
+    int4 *g = reinterpret_cast<int4 *>(b.vel_grid);
+    b.vel_flat[c] = g[c];
+    g[c] = make_int4(0, 0, 0, 0);
+}
+
+__device__ __forceinline__ void store_tracer(const DevParams &P, uint32_t *tr, uint32_t i, F3 pos,
+                                             float speed) {  // :75-80
+    const float ux = clampf((pos.x - P.tracer_c[0]) / P.tracer_e[0] * 0.5f + 0.5f, 0.0f, 1.0f);
+    const float uy = clampf((pos.y - P.tracer_c[1]) / P.tracer_e[1] * 0.5f + 0.5f, 0.0f, 1.0f);
+    const uint32_t qx = (uint32_t)(ux * 65535.0f + 0.5f);
+    const uint32_t qy = (uint32_t)(uy * 65535.0f + 0.5f);
+    const uint32_t hz = __half_as_ushort(__float2half_rn(pos.z - P.tracer_c[2]));
+    const uint32_t hs = __half_as_ushort(__float2half_rn(speed));
+    reinterpret_cast<uint2 *>(tr)[i] = make_uint2(qx | (qy << 16), hz | (hs << 16));
+}
+
+__device__ __forceinline__ F3 tracer_clamp(const DevParams &P, F3 v) {
+    return f3(clampf(v.x, P.tracer_c[0] - P.tracer_e[0], P.tracer_c[0] + P.tracer_e[0]),
+              clampf(v.y, P.tracer_c[1] - P.tracer_e[1], P.tracer_c[1] + P.tracer_e[1]),
+              clampf(v.z, P.tracer_c[2] - P.tracer_e[2], P.tracer_c[2] + P.tracer_e[2]));
+}
+
+__device__ void respawn(const DevParams &P, const SimBufs &b, uint32_t slot, uint32_t r) {  // :82-92
+    const uint32_t r1 = pcg(r), r2 = pcg(r1), r3 = pcg(r2), r4 = pcg(r3);
+    const float half_cell = P.cell * 0.5f;
+    const F3 jit = f3(((float)(r2 >> 20) / 4096.0f - 0.5f) * half_cell,
+                      ((float)(r3 >> 20) / 4096.0f - 0.5f) * half_cell,
+                      ((float)(r4 >> 20) / 4096.0f - 0.5f) * half_cell);
+    const uint32_t j = r1 % P.count;
+    store_tracer(P, b.tracers, slot, tracer_clamp(P, xyz(b.pos[j]) + jit), len(xyz(b.vel[j])));
+}
+
+__global__ void __launch_bounds__(256) k_advect(DevParams P, SimBufs b, DevStep stv,
+                                                uint32_t ntr) {  // :140-183
+    const DevStep *stp = &stv;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ntr) return;
+    const float dt = stp->s.dt;
+    const float p_respawn = dt / 3.0f;
+    const float p_stray = dt / 0.25f;
+    const uint32_t r0 = pcg(i ^ pcg(stp->s.seed));
+    if ((float)r0 / 4294967296.0f < p_respawn) {
+        respawn(P, b, i, r0);
+        return;
+    }
+    const uint2 t = reinterpret_cast<const uint2 *>(b.tracers)[i];
+    float old[4];
+    old[0] = ((float)(t.x & 0xffffu) / 65535.0f * 2.0f - 1.0f) * P.tracer_e[0] + P.tracer_c[0];
+    old[1] = ((float)(t.x >> 16) / 65535.0f * 2.0f - 1.0f) * P.tracer_e[1] + P.tracer_c[1];
+    old[2] = __half2float(__ushort_as_half((unsigned short)(t.y & 0xffffu))) + P.tracer_c[2];
+    old[3] = __half2float(__ushort_as_half((unsigned short)(t.y >> 16)));
+    F3 pos = f3(old[0], old[1], old[2]);
+    const float gp[3] = {(pos.x - P.box_min[0]) / P.cell - 0.5f, (pos.y - P.box_min[1]) / P.cell - 0.5f,
+                         (pos.z - P.box_min[2]) / P.cell - 0.5f};
+    uint32_t base[3];
+    float f[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        int32_t bi = __float2int_rz(floorf(gp[a]));
+        const int32_t top = (int32_t)P.dims[a] - 2;
+        bi = bi < 0 ? 0 : (bi > top ? top : bi);
+        base[a] = (uint32_t)bi;
+        f[a] = clampf(gp[a] - (float)base[a], 0.0f, 1.0f);
+    }
+    float mx = 0.0f, my = 0.0f, mz = 0.0f, wc = 0.0f;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) {
+        const uint32_t ox = k & 1u, oy = (k >> 1) & 1u, oz = (k >> 2) & 1u;
+        const float wx = ox ? f[0] : 1.0f - f[0];
+        const float wy = oy ? f[1] : 1.0f - f[1];
+        const float wz = oz ? f[2] : 1.0f - f[2];
+        const float weight = wx * wy * wz;
+        const uint32_t c = ((base[2] + oz) * P.dims[1] + (base[1] + oy)) * P.dims[0] + (base[0] + ox);
+        const int4 cell = b.vel_flat[c];
+        mx += weight * (float)cell.x;
+        my += weight * (float)cell.y;
+        mz += weight * (float)cell.z;
+        wc += weight * (float)cell.w;
+    }
+    F3 v = f3(0.f, 0.f, 0.f);
+    if (wc > 0.0f) {
+        const float den = wc * 65536.0f;
+        v = f3(mx / den, my / den, mz / den);
+    } else if ((float)pcg(r0 ^ 0x85ebca6bu) / 4294967296.0f < p_stray) {
+        respawn(P, b, i, pcg(r0 ^ 0x632be59bu));
+        return;
+    }
+    pos = pos + v * dt;
+    store_tracer(P, b.tracers, i, tracer_clamp(P, pos), fmaxf(len(v), old[3] * stp->decay));
+}
+
+inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
+
+}  // namespace
+
+void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n) {
+    k_gather<<<blocks_for(n, 256), 256, 0, s>>>(b, n);
+}
+void launch_density_div(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                        DevSolve *solve, unsigned long long *acc) {
+    k_density_div<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, solve, acc);
+}
+void launch_div_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                      unsigned long long *acc) {
+    k_div_kappa<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, acc);
+}
+void launch_apply(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                  bool add_pressure) {
+    k_apply<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, add_pressure ? 1 : 0);
+}
+void launch_forces_eval(cudaStream_t s, const DevParams &P, const SimBufs &b) {
+    k_forces_eval<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b);
+}
+void launch_forces_apply(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st) {
+    k_forces_apply<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st);
+}
+void launch_den_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                      unsigned long long *acc) {
+    k_den_kappa<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, acc);
+}
+void launch_integrate(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                      DevSolve *solve, int div_slot, int den_slot, int div_iters, int den_iters) {
+    k_integrate<<<blocks_for(P.count, 256), 256, 0, s>>>(P, b, st, solve, div_slot, den_slot,
+                                                         div_iters, den_iters);
+}
+void launch_finish_residual(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int count_iter,
+                            int reset_iters) {
+    k_finish_residual<<<1, 1, 0, s>>>(solve, n, which, count_iter, reset_iters);
+}
+void launch_stats(cudaStream_t s, const DevParams &P, const SimBufs &b, DevSolve *solve) {
+    uint32_t blocks = blocks_for(P.count, kStatsThreads);
+    if (blocks > kStatsBlocks) blocks = kStatsBlocks;
+    k_stats_partial<<<blocks, kStatsThreads, 0, s>>>(P, b);
+    k_stats_final<<<1, 32, 0, s>>>(P, b, solve, blocks);
+}
+void launch_splat(cudaStream_t s, const DevParams &P, const SimBufs &b) {
+    k_splat<<<blocks_for(P.count, 256), 256, 0, s>>>(P, b);
+}
+void launch_resolve(cudaStream_t s, const DevParams &P, const SimBufs &b) {
+    const uint32_t cells = P.dims[0] * P.dims[1] * P.dims[2];
+    k_resolve<<<blocks_for(cells, 256), 256, 0, s>>>(b, cells);
+}
+void launch_advect(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep &st,
+                   uint32_t ntr) {
+    if (ntr) k_advect<<<blocks_for(ntr, 256), 256, 0, s>>>(P, b, st, ntr);
+}
+
+}  // namespace fcu

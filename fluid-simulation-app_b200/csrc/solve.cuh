@@ -1,0 +1,62 @@
+// solve.cuh — the DFSPH substep's sweeps, integrate, statistics, tracers.
+#pragma once
+
+#include "common.cuh"
+
+namespace fcu {
+
+// Device pointers of one box's particle state and scratch.
+struct SimBufs {
+    // resting set (slot order of the last integrate)
+    float4 *pos, *vel, *pvel;
+    float *pp, *temp;
+    uint32_t *id;
+    // working set (this substep's cell order)
+    float4 *wpos, *wvel, *wpvel;
+    float *wpp, *wtemp;
+    uint32_t *wid;
+    // scratch
+    uint32_t *keys, *starts, *perm;
+    float *density, *alpha, *kd, *pressure, *pinc, *rho_near;
+    float4 *accel, *xsph, *wgrad;
+    uint32_t *nbr, *nbr_n;
+    // tracers
+    uint32_t *tracers;  // 2 words each
+    int32_t *vel_grid;  // 4 per cell, atomic sums
+    int4 *vel_flat;
+    // stats
+    float *stats_part;  // [blocks][12]
+    unsigned long long *stats_acc;
+    float *stats;       // 14
+};
+
+constexpr int kSolveThreads = 128;
+constexpr int kStatsBlocks = 148;
+constexpr int kStatsThreads = 256;
+
+// Enqueue helpers: each launches one kernel on `s`.
+void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n);
+void launch_density_div(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                        DevSolve *solve, unsigned long long *acc);
+void launch_div_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                      unsigned long long *acc);
+void launch_apply(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                  bool add_pressure);
+void launch_forces_eval(cudaStream_t s, const DevParams &P, const SimBufs &b);
+void launch_forces_apply(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st);
+void launch_den_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                      unsigned long long *acc);
+void launch_integrate(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
+                      DevSolve *solve, int div_slot, int den_slot, int div_iters, int den_iters);
+// Residual bookkeeping after a sweep that accumulated one: which = 0
+// divergence, 1 density. Records the residual, bumps the iteration count
+// when `count_iter`, clears the accumulator.
+void launch_finish_residual(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int count_iter,
+                            int reset_iters);
+void launch_stats(cudaStream_t s, const DevParams &P, const SimBufs &b, DevSolve *solve);
+void launch_splat(cudaStream_t s, const DevParams &P, const SimBufs &b);
+void launch_resolve(cudaStream_t s, const DevParams &P, const SimBufs &b);
+void launch_advect(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep &st,
+                   uint32_t ntr);
+
+}  // namespace fcu

@@ -1,0 +1,347 @@
+"""ctypes binding of libfluidcu.so (include/fluid_cu.h).
+
+The host-side view of the C ABI that tests, the benchmark and any Python
+caller use. It mirrors the reference's sim-facing interface (Renderer::new /
+frame / stats / set_particles, crates/fluid-core/src/render.rs:2801-3576, and
+the C ABI of crates/fluid-ffi) minus drawing. There is no CPU fallback: if
+the CUDA library is missing this module raises on import of the library.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfluidcu.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "fluid_cu.h")
+
+OK, ERR_ARG, ERR_CUDA, ERR_TIMEOUT, ERR_NAN, ERR_STATE, ERR_OOM = 0, -1, -2, -3, -4, -5, -6
+GEOMETRY_SLAB, GEOMETRY_BOX = 0, 1
+SEED_SLAB, SEED_BLOCK, SEED_NONE = 0, 1, 2
+SOLVE_FIXED, SOLVE_TOLERANCE = 0, 1
+FIELDS = dict(density=0, alpha=1, kd=2, pressure=3, nbr_n=4, starts=5, perm=6, work_pos=7,
+              work_vel=8, accel=9, xsph=10, wall_grad=11, counters=12)
+
+
+class FluidVec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
+class FluidStep(C.Structure):
+    _fields_ = [("force", C.c_float * 3), ("dt", C.c_float), ("omega", C.c_float * 3),
+                ("v_clamp", C.c_float), ("domega", C.c_float * 3), ("seed", C.c_uint32),
+                ("touch_r", C.c_float), ("touch_n", C.c_uint32), ("pad", C.c_uint32 * 2),
+                ("touches", (C.c_float * 4) * 5)]
+
+
+class FluidSimConfig(C.Structure):
+    _fields_ = [("geometry", C.c_uint32), ("extent", C.c_float * 2), ("box_lo", C.c_float * 3),
+                ("box_hi", C.c_float * 3), ("spacing", C.c_float), ("h_ratio", C.c_float),
+                ("rest_density", C.c_float), ("seeding", C.c_uint32), ("fill", C.c_float),
+                ("block", C.c_uint32 * 3), ("jitter", C.c_float), ("seed", C.c_uint64),
+                ("count", C.c_uint32), ("tracers", C.c_uint32), ("xsph_blend", C.c_float),
+                ("temperature", C.c_float), ("solve", C.c_uint32), ("div_iters", C.c_uint32),
+                ("den_iters", C.c_uint32), ("div_tol", C.c_float), ("den_tol", C.c_float),
+                ("max_iters", C.c_uint32), ("nbr_cap", C.c_uint32), ("device", C.c_int32)]
+
+
+class FluidSimParams(C.Structure):
+    _fields_ = [("box_min", C.c_float * 3), ("cell", C.c_float), ("dims", C.c_uint32 * 3),
+                ("count", C.c_uint32), ("h", C.c_float), ("mass", C.c_float),
+                ("rho0", C.c_float), ("inv_h", C.c_float), ("sigma", C.c_float),
+                ("sigma_h", C.c_float), ("support_sq", C.c_float), ("wall_lo", C.c_float * 3),
+                ("wall_hi", C.c_float * 3), ("tracer_c", C.c_float * 3),
+                ("tracer_e", C.c_float * 3), ("xsph_blend", C.c_float), ("nbr_cap", C.c_uint32)]
+
+
+class FluidSimStats(C.Structure):
+    _fields_ = [("compression_avg", C.c_float), ("compression_max", C.c_float),
+                ("density_min", C.c_float), ("density_max", C.c_float),
+                ("pressure_min", C.c_float), ("pressure_max", C.c_float), ("v_max", C.c_float),
+                ("temperature_min", C.c_float), ("temperature_max", C.c_float),
+                ("clamp_count", C.c_uint32), ("neighbour_overflow", C.c_uint32),
+                ("v_min", C.c_float), ("accel_min", C.c_float), ("accel_max", C.c_float),
+                ("div_iters", C.c_uint32), ("den_iters", C.c_uint32),
+                ("div_residual", C.c_double), ("den_residual", C.c_double),
+                ("substeps", C.c_uint64), ("substeps_last_frame", C.c_uint32),
+                ("error", C.c_int32)]
+
+    def as_reference_block(self):
+        """The 14-float stats block of sim_solve.wgsl:800-874, in its slot order."""
+        return np.array([self.compression_avg, self.compression_max, self.density_min,
+                         self.density_max, self.pressure_min, self.pressure_max, self.v_max,
+                         self.temperature_min, self.temperature_max, float(self.clamp_count),
+                         float(self.neighbour_overflow), self.v_min, self.accel_min,
+                         self.accel_max], np.float32)
+
+
+class FluidGrid(C.Structure):
+    _fields_ = [("min", C.c_float * 3), ("cell", C.c_float), ("dims", C.c_uint32 * 3)]
+
+
+assert C.sizeof(FluidStep) == 144
+
+
+def header_functions():
+    """Names of the functions include/fluid_cu.h declares."""
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fluid_[a-z0-9_]+)\s*\(", text)))
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it (make -C fluid-simulation-app_b200); "
+                           "there is no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    P = C.c_void_p
+    vp = C.c_void_p
+    i32, u32, u64, f = C.c_int32, C.c_uint32, C.c_uint64, C.c_float
+    sig = {
+        "fluid_last_error": (C.c_char_p, []),
+        "fluid_sim_default_config": (None, [C.POINTER(FluidSimConfig)]),
+        "fluid_sim_create": (P, [C.POINTER(FluidSimConfig)]),
+        "fluid_sim_destroy": (None, [P]),
+        "fluid_sim_params": (i32, [P, C.POINTER(FluidSimParams)]),
+        "fluid_sim_count": (u32, [P]),
+        "fluid_sim_tracer_count": (u32, [P]),
+        "fluid_sim_stream": (vp, [P]),
+        "fluid_sim_step": (i32, [P, C.POINTER(FluidStep)]),
+        "fluid_sim_run": (i32, [P, C.POINTER(FluidStep), u32]),
+        "fluid_sim_reduce_stats": (i32, [P]),
+        "fluid_sim_tracers": (i32, [P, C.POINTER(FluidStep)]),
+        "fluid_sim_advect": (i32, [P, C.POINTER(FluidStep)]),
+        "fluid_sim_frame": (i32, [P, FluidVec3, FluidVec3, FluidVec3, f, u32, u32, u32]),
+        "fluid_sim_sync": (i32, [P]),
+        "fluid_sim_stats": (i32, [P, C.POINTER(FluidSimStats)]),
+        "fluid_sim_get_state": (i32, [P, vp, vp, vp, vp, vp, vp]),
+        "fluid_sim_set_state": (i32, [P, vp, vp, vp, vp, vp, vp]),
+        "fluid_sim_read_particles": (i32, [P, vp, vp]),
+        "fluid_sim_get_tracers": (i32, [P, vp]),
+        "fluid_sim_set_tracers": (i32, [P, vp]),
+        "fluid_sim_read_field": (i32, [P, i32, vp, u64]),
+        "fluid_sim_profile_step": (i32, [P, C.POINTER(FluidStep), C.POINTER(f),
+                                         C.POINTER(C.c_char_p), u32]),
+        "fluid_sim_kernels_per_substep": (u32, [P]),
+        "fluid_grid_workspace_bytes": (u64, [u32, C.POINTER(FluidGrid)]),
+        "fluid_grid_build": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp, u64, vp]),
+        "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+class FluidError(RuntimeError):
+    def __init__(self, code, what):
+        super().__init__(f"{what}: status {code}: {last_error()}")
+        self.code = code
+
+
+def last_error():
+    return lib().fluid_last_error().decode()
+
+
+def check(rc, what):
+    if rc != OK:
+        raise FluidError(rc, what)
+    return rc
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def default_config(**kw):
+    cfg = FluidSimConfig()
+    lib().fluid_sim_default_config(C.byref(cfg))
+    for k, v in kw.items():
+        fld = getattr(cfg, k)
+        if isinstance(fld, C.Array):
+            fld[:] = list(v)
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+def make_step(force=(0.0, 0.0, 0.0), dt=0.0, omega=(0.0, 0.0, 0.0), v_clamp=0.0,
+              domega=(0.0, 0.0, 0.0), seed=0, touch_r=0.0, touches=()):
+    """pack_step (sim.rs:215-252) as a struct."""
+    st = FluidStep()
+    st.force[:] = [float(v) for v in force]
+    st.dt = dt
+    st.omega[:] = [float(v) for v in omega]
+    st.v_clamp = v_clamp
+    st.domega[:] = [float(v) for v in domega]
+    st.seed = seed
+    st.touch_r = touch_r
+    st.touch_n = len(touches)
+    for i, t in enumerate(touches):
+        st.touches[i][:] = [float(v) for v in t]
+    return st
+
+
+class Sim:
+    """One box of fluid on one GPU: the handle of fluid_sim_create."""
+
+    def __init__(self, cfg=None, **kw):
+        if cfg is None:
+            cfg = default_config(**kw)
+        self.cfg = cfg
+        h = lib().fluid_sim_create(C.byref(cfg))
+        if not h:
+            raise FluidError(ERR_ARG, "fluid_sim_create")
+        self.h = h
+        self.n = lib().fluid_sim_count(h)
+        self.ntr = lib().fluid_sim_tracer_count(h)
+        self.params = FluidSimParams()
+        check(lib().fluid_sim_params(h, C.byref(self.params)), "params")
+        d = self.params.dims
+        self.cells = d[0] * d[1] * d[2]
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fluid_sim_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def step(self, st):
+        return check(lib().fluid_sim_step(self.h, C.byref(st)), "step")
+
+    def run(self, steps):
+        arr = (FluidStep * len(steps))(*steps)
+        return check(lib().fluid_sim_run(self.h, arr, len(steps)), "run")
+
+    def reduce_stats(self):
+        return check(lib().fluid_sim_reduce_stats(self.h), "reduce_stats")
+
+    def tracers_pass(self, st):
+        return check(lib().fluid_sim_tracers(self.h, C.byref(st)), "tracers")
+
+    def advect(self, st):
+        return check(lib().fluid_sim_advect(self.h, C.byref(st)), "advect")
+
+    def frame(self, force, dt, omega=(0, 0, 0), domega=(0, 0, 0), substeps=0, cap=16, seed=0):
+        v = lambda t: FluidVec3(*[float(x) for x in t])
+        return check(lib().fluid_sim_frame(self.h, v(force), v(omega), v(domega), dt, substeps,
+                                           cap, seed), "frame")
+
+    def sync(self):
+        return check(lib().fluid_sim_sync(self.h), "sync")
+
+    def stats(self, allow_error=False):
+        st = FluidSimStats()
+        rc = lib().fluid_sim_stats(self.h, C.byref(st))
+        if not allow_error:
+            check(rc, "stats")
+        return st
+
+    def state(self):
+        n = self.n
+        out = dict(pos=np.zeros((n, 4), np.float32), vel=np.zeros((n, 4), np.float32),
+                   prev_vel=np.zeros((n, 4), np.float32), prev_p=np.zeros(n, np.float32),
+                   temp=np.zeros(n, np.float32), id=np.zeros(n, np.uint32))
+        check(lib().fluid_sim_get_state(self.h, *[_p(out[k]) for k in
+                                                  ("pos", "vel", "prev_vel", "prev_p", "temp",
+                                                   "id")]), "get_state")
+        return out
+
+    def set_state(self, pos4=None, vel4=None, prev_vel4=None, prev_p=None, temp=None, ids=None):
+        c = lambda a, dt: None if a is None else np.ascontiguousarray(a, dt)
+        arrs = [c(pos4, np.float32), c(vel4, np.float32), c(prev_vel4, np.float32),
+                c(prev_p, np.float32), c(temp, np.float32), c(ids, np.uint32)]
+        return check(lib().fluid_sim_set_state(self.h, *[_p(a) for a in arrs]), "set_state")
+
+    def read_particles(self):
+        pos = np.zeros((self.n, 4), np.float32)
+        vel = np.zeros((self.n, 4), np.float32)
+        check(lib().fluid_sim_read_particles(self.h, _p(pos), _p(vel)), "read_particles")
+        return pos, vel
+
+    def tracers(self):
+        out = np.zeros((max(self.ntr, 0), 2), np.uint32)
+        check(lib().fluid_sim_get_tracers(self.h, _p(out)), "get_tracers")
+        return out
+
+    def set_tracers(self, packed):
+        packed = np.ascontiguousarray(packed, np.uint32)
+        check(lib().fluid_sim_set_tracers(self.h, _p(packed)), "set_tracers")
+
+    def field(self, name):
+        n = self.n
+        shapes = dict(density=(n, np.float32), alpha=(n, np.float32), kd=(n, np.float32),
+                      pressure=(n, np.float32), nbr_n=(n, np.uint32),
+                      starts=(self.cells + 1, np.uint32), perm=(n, np.uint32),
+                      work_pos=((n, 4), np.float32), work_vel=((n, 4), np.float32),
+                      accel=((n, 4), np.float32), xsph=((n, 4), np.float32),
+                      wall_grad=((n, 4), np.float32), counters=(2, np.uint32))
+        shape, dt = shapes[name]
+        out = np.zeros(shape, dt)
+        check(lib().fluid_sim_read_field(self.h, FIELDS[name], _p(out), out.nbytes), name)
+        return out
+
+    def profile_step(self, st, cap=128):
+        ms = (C.c_float * cap)()
+        names = (C.c_char_p * cap)()
+        k = lib().fluid_sim_profile_step(self.h, C.byref(st), ms, names, cap)
+        if k < 0:
+            raise FluidError(k, "profile_step")
+        return [(names[i].decode(), ms[i]) for i in range(k)]
+
+    def kernels_per_substep(self):
+        return lib().fluid_sim_kernels_per_substep(self.h)
+
+    def stream(self):
+        return lib().fluid_sim_stream(self.h)
+
+
+def grid_of(params):
+    g = FluidGrid()
+    g.min[:] = list(params.box_min) if hasattr(params, "box_min") else list(params.min)
+    g.cell = params.cell
+    g.dims[:] = list(params.dims)
+    return g
+
+
+def grid_build_host(pos4, grid):
+    """fluid_grid_build_host: (starts[C+1], perm[n]) for host positions."""
+    pos4 = np.ascontiguousarray(pos4, np.float32).reshape(-1, 4)
+    n = pos4.shape[0]
+    C_ = grid.dims[0] * grid.dims[1] * grid.dims[2]
+    starts = np.zeros(C_ + 1, np.uint32)
+    perm = np.zeros(n, np.uint32)
+    check(lib().fluid_grid_build_host(_p(pos4), n, C.byref(grid), _p(starts), _p(perm)),
+          "grid_build_host")
+    return starts, perm
+
+
+def grid_build_device(pos4_ptr, n, grid, keys_ptr, starts_ptr, perm_ptr, ws_ptr, ws_bytes,
+                      stream=None):
+    """fluid_grid_build on device pointers (ints, e.g. torch data_ptr())."""
+    return check(lib().fluid_grid_build(C.c_void_p(pos4_ptr), n, C.byref(grid),
+                                        C.c_void_p(keys_ptr) if keys_ptr else None,
+                                        C.c_void_p(starts_ptr), C.c_void_p(perm_ptr),
+                                        C.c_void_p(ws_ptr), ws_bytes,
+                                        C.c_void_p(stream) if stream else None), "grid_build")
+
+
+def grid_workspace_bytes(n, grid):
+    return lib().fluid_grid_workspace_bytes(n, C.byref(grid))

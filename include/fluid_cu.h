@@ -1,0 +1,276 @@
+/*
+ * fluid_cu.h — C ABI of the B200 DFSPH step (libfluidcu.so).
+ *
+ * The drop-in boundary for fluid-core's per-frame simulation step. It keeps
+ * the conventions of the reference's C ABI (crates/fluid-ffi/include/
+ * fluid_ffi.h:11-182, crates/fluid-ffi/src/lib.rs:72-285): an opaque handle,
+ * plain-old-data structs passed by value or pointer, create returning null
+ * with the reason available as text. Rendering and surfaces are not part of
+ * it. Unlike the reference, every call that can fail returns a status code.
+ *
+ * Threading: one handle per host thread. Calls are ordered on the handle's
+ * CUDA stream and return before the GPU finishes, except those documented
+ * as synchronising (stats, reads, sync).
+ */
+#ifndef FLUID_CU_H
+#define FLUID_CU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define FLUID_OK 0
+#define FLUID_ERR_ARG -1     /* bad argument or size */
+#define FLUID_ERR_CUDA -2    /* a CUDA call failed; see fluid_last_error() */
+#define FLUID_ERR_TIMEOUT -3 /* a bounded device-side wait gave up */
+#define FLUID_ERR_NAN -4     /* a non-finite value reached the statistics */
+#define FLUID_ERR_STATE -5   /* call not valid in the handle's state */
+#define FLUID_ERR_OOM -6     /* device allocation failed */
+
+/* Replaces fluid_ffi.h:58 FLUID_TOUCH_SLOTS; sim.rs:180 MAX_TOUCHES. */
+#define FLUID_TOUCH_SLOTS 5
+/* sim_solve.wgsl:388 NBR_CAP. */
+#define FLUID_NBR_CAP_DEFAULT 96
+
+typedef struct FluidSim FluidSim;
+
+/* fluid_ffi.h:17-21 */
+typedef struct FluidVec3 {
+    float x;
+    float y;
+    float z;
+} FluidVec3;
+
+/* The 144-byte Step block, byte for byte: sim.rs:200-252 (pack_step),
+ * sim_solve.wgsl:29-41. force is the body force (tilt gravity), m/s^2 in the
+ * box frame; dt the substep; omega / domega the box's angular velocity and
+ * acceleration; v_clamp the CFL speed; seed the tracer seed; the fingers'
+ * shared radius, count and (x, y, vx, vy) each. */
+typedef struct FluidStep {
+    float force[3];
+    float dt;
+    float omega[3];
+    float v_clamp;
+    float domega[3];
+    uint32_t seed;
+    float touch_r;
+    uint32_t touch_n;
+    uint32_t pad[2];
+    float touches[FLUID_TOUCH_SLOTS][4];
+} FluidStep;
+
+#define FLUID_GEOMETRY_SLAB 0 /* the reference slab: +-extent in x, y; +-slab depth/2 in z */
+#define FLUID_GEOMETRY_BOX 1  /* any axis-aligned box [box_lo, box_hi] */
+
+#define FLUID_SEED_SLAB 0  /* sim.rs:77-100 seed_slab at `fill` */
+#define FLUID_SEED_BLOCK 1 /* lattice block of `block` dims at box_lo, splitmix64 jitter */
+#define FLUID_SEED_NONE 2  /* `count` particles at the origin until set_state */
+
+#define FLUID_SOLVE_FIXED 0     /* div_iters / den_iters applies (reference: 1 / 5) */
+#define FLUID_SOLVE_TOLERANCE 1 /* iterate to div_tol / den_tol, FP64 residuals, capped */
+
+/* What fluid_renderer_create's sim arguments (fluid_ffi.h:74-83) and
+ * Sim::new (render.rs:1468-1612) decide, made explicit. */
+typedef struct FluidSimConfig {
+    uint32_t geometry;
+    float extent[2]; /* slab half width and height, m */
+    float box_lo[3]; /* box corners, m */
+    float box_hi[3];
+    float spacing;      /* lattice spacing d, m */
+    float h_ratio;      /* kernel h / d; the reference uses 1.2 (render.rs:1477) */
+    float rest_density; /* kg/m^3; 0 selects the reference's 998.2 (sim.rs:6) */
+    uint32_t seeding;
+    float fill;         /* seed_slab's height fraction (0.5 in the reference) */
+    uint32_t block[3];  /* FLUID_SEED_BLOCK lattice dims */
+    float jitter;       /* FLUID_SEED_BLOCK jitter amplitude, fraction of d */
+    uint64_t seed;      /* FLUID_SEED_BLOCK stream seed */
+    uint32_t count;     /* FLUID_SEED_NONE particle count */
+    uint32_t tracers;   /* passive tracers, seeded as sim.rs:105-122 */
+    float xsph_blend;   /* < 0: the reference's 1 - exp(-6 dt) per substep */
+    float temperature;  /* initial K (293.15 in the reference) */
+    uint32_t solve;
+    uint32_t div_iters;
+    uint32_t den_iters;
+    float div_tol;      /* mean positive divergence * dt / rho0 */
+    float den_tol;      /* mean positive predicted compression */
+    uint32_t max_iters;
+    uint32_t nbr_cap;   /* neighbours kept per particle (overflow counted) */
+    int32_t device;     /* CUDA device ordinal */
+} FluidSimConfig;
+
+/* The derived constants every kernel reads (SimParams, sim_solve.wgsl:11-23,
+ * plus the walls and tracer box made explicit). */
+typedef struct FluidSimParams {
+    float box_min[3];
+    float cell;
+    uint32_t dims[3];
+    uint32_t count;
+    float h, mass, rho0, inv_h, sigma, sigma_h, support_sq;
+    float wall_lo[3];
+    float wall_hi[3];
+    float tracer_c[3];
+    float tracer_e[3];
+    float xsph_blend;
+    uint32_t nbr_cap;
+} FluidSimParams;
+
+/* The reduce_stats block (sim_solve.wgsl:800-874; the sim half of
+ * FluidRenderStats, fluid_ffi.h:23-47) plus the solver's own counters. */
+typedef struct FluidSimStats {
+    float compression_avg; /* mean max(rho/rho0 - 1, 0): the density error */
+    float compression_max;
+    float density_min;
+    float density_max;
+    float pressure_min;
+    float pressure_max;
+    float v_max;
+    float temperature_min;
+    float temperature_max;
+    uint32_t clamp_count;        /* cumulative CFL clamps */
+    uint32_t neighbour_overflow; /* cumulative neighbours past nbr_cap */
+    float v_min;
+    float accel_min;
+    float accel_max;
+    uint32_t div_iters;    /* last substep */
+    uint32_t den_iters;    /* last substep, warm start excluded */
+    double div_residual;   /* last substep, after its last divergence apply */
+    double den_residual;   /* last substep, after its last density apply */
+    uint64_t substeps;     /* substeps run since create */
+    uint32_t substeps_last_frame;
+    int32_t error;         /* sticky device error (FLUID_ERR_*) */
+} FluidSimStats;
+
+/* Internal buffers a test may read back (render.rs tests read starts,
+ * density and the working set the same way). */
+#define FLUID_FIELD_DENSITY 0   /* float[n], working order */
+#define FLUID_FIELD_ALPHA 1
+#define FLUID_FIELD_KD 2
+#define FLUID_FIELD_PRESSURE 3
+#define FLUID_FIELD_NBR_N 4     /* uint32[n] */
+#define FLUID_FIELD_STARTS 5    /* uint32[C+1] */
+#define FLUID_FIELD_PERM 6      /* uint32[n] */
+#define FLUID_FIELD_WORK_POS 7  /* float4[n] */
+#define FLUID_FIELD_WORK_VEL 8  /* float4[n] */
+#define FLUID_FIELD_ACCEL 9     /* float4[n] */
+#define FLUID_FIELD_XSPH 10     /* float4[n] */
+#define FLUID_FIELD_WALL_GRAD 11
+#define FLUID_FIELD_COUNTERS 12 /* uint32[2]: clamp count, neighbour overflow */
+
+/* Text of the last error on this thread ("" if none). */
+const char *fluid_last_error(void);
+
+/* The reference's defaults: slab geometry, seed_slab at fill 0.5, h = 1.2 d,
+ * rest density 998.2, 293.15 K, fixed schedule 1 / 5, 96 neighbours. */
+void fluid_sim_default_config(FluidSimConfig *cfg);
+
+/* Replaces fluid_renderer_create (fluid_ffi.h:74-83; lib.rs:72-109) for the
+ * sim alone: builds the particles, the grid and every device buffer, and
+ * captures the substep as a CUDA graph. Null on failure, reason in
+ * fluid_last_error() and on stderr. */
+FluidSim *fluid_sim_create(const FluidSimConfig *cfg);
+
+/* Replaces fluid_renderer_destroy (fluid_ffi.h:182; lib.rs:283-285). */
+void fluid_sim_destroy(FluidSim *sim);
+
+int32_t fluid_sim_params(const FluidSim *sim, FluidSimParams *out);
+uint32_t fluid_sim_count(const FluidSim *sim);
+uint32_t fluid_sim_tracer_count(const FluidSim *sim);
+/* The handle's cudaStream_t. */
+void *fluid_sim_stream(FluidSim *sim);
+
+/* One substep (render.rs:3175-3202 per substep): rebuild, density and
+ * factor, the divergence solve, forces, the constant-density solve,
+ * integrate. dt == 0 runs the rebuild and the density sweep alone, as the
+ * reference's zero-substep test path (render.rs:3904-3955). Asynchronous. */
+int32_t fluid_sim_step(FluidSim *sim, const FluidStep *step);
+
+/* `n` substeps from an array of Step blocks, one upload. Asynchronous. */
+int32_t fluid_sim_run(FluidSim *sim, const FluidStep *steps, uint32_t n);
+
+/* reduce_stats on the current state (render.rs:3203). Asynchronous. */
+int32_t fluid_sim_reduce_stats(FluidSim *sim);
+
+/* One tracer pass (splat, resolve, advect; render.rs:3204-3228) with the
+ * frame's dt and seed from `step`. Asynchronous. */
+int32_t fluid_sim_tracers(FluidSim *sim, const FluidStep *step);
+/* advect alone on the last resolved field (render.rs:5770-5787). */
+int32_t fluid_sim_advect(FluidSim *sim, const FluidStep *step);
+
+/* One frame the way Renderer::frame encodes it (render.rs:3090-3228), minus
+ * drawing: `substeps` substeps of dt/substeps (0 selects substeps_for on the
+ * last frame's v_max, capped at `cap`), v_clamp = 0.4 d / dt_sub, refine
+ * passes by refine_passes(dt_sub) in the fixed schedule, then reduce_stats
+ * and, with tracers, one tracer pass at the frame dt and `seed`. A dt of 0
+ * encodes nothing (render.rs:3165-3168). Asynchronous; the stats it uses
+ * for v_max are the previous frame's, read without blocking. */
+int32_t fluid_sim_frame(FluidSim *sim, FluidVec3 force, FluidVec3 omega, FluidVec3 domega,
+                        float dt, uint32_t substeps, uint32_t cap, uint32_t seed);
+
+/* Waits for the handle's stream. Returns a sticky device error if one was
+ * raised (a bounded wait that gave up). */
+int32_t fluid_sim_sync(FluidSim *sim);
+
+/* Replaces fluid_renderer_stats (fluid_ffi.h:175): the last reduce_stats
+ * plus the solver counters. Synchronises. */
+int32_t fluid_sim_stats(FluidSim *sim, FluidSimStats *out);
+
+/* The resting set in slot order, any pointer may be null. Synchronises. */
+int32_t fluid_sim_get_state(FluidSim *sim, float *pos4, float *vel4, float *prev_vel4,
+                            float *prev_p, float *temp, uint32_t *id);
+/* Replaces the resting set; null pointers leave that record unchanged.
+ * Resets the warm start and the counters' baselines nowhere: the state is
+ * taken as is. */
+int32_t fluid_sim_set_state(FluidSim *sim, const float *pos4, const float *vel4,
+                            const float *prev_vel4, const float *prev_p, const float *temp,
+                            const uint32_t *id);
+/* Positions and velocities ordered by particle id (the seed's order): the
+ * particle-readback interface. Synchronises. */
+int32_t fluid_sim_read_particles(FluidSim *sim, float *pos4, float *vel4);
+
+/* Tracers as packed 8-byte records (sim_tracers.wgsl:64-80). */
+int32_t fluid_sim_get_tracers(FluidSim *sim, uint32_t *packed2);
+int32_t fluid_sim_set_tracers(FluidSim *sim, const uint32_t *packed2);
+
+/* Copies an internal buffer (FLUID_FIELD_*) to host memory. Synchronises. */
+int32_t fluid_sim_read_field(FluidSim *sim, int32_t field, void *out, uint64_t bytes);
+
+/* Times one substep kernel by kernel with CUDA events on the handle's
+ * stream: writes up to `cap` durations (ms) and names, returns the count. */
+int32_t fluid_sim_profile_step(FluidSim *sim, const FluidStep *step, float *ms,
+                               const char **names, uint32_t cap);
+/* Kernel launches one substep issues at the current schedule (fixed mode). */
+uint32_t fluid_sim_kernels_per_substep(const FluidSim *sim);
+
+/* ---- the neighbour grid alone ------------------------------------------ */
+
+/* Grid geometry: sim.rs:14-44 (Grid). Key of a position:
+ * (z * dims.y + y) * dims.x + x of min(u32((p - min) / cell), dims - 1). */
+typedef struct FluidGrid {
+    float min[3];
+    float cell;
+    uint32_t dims[3];
+} FluidGrid;
+
+/* Device workspace bytes fluid_grid_build needs for n positions. */
+uint64_t fluid_grid_workspace_bytes(uint32_t n, const FluidGrid *grid);
+
+/* The counting sort of sim_grid.wgsl:44-72 and sim_density.wgsl:36-55 with
+ * the scan of sim_scan.wgsl:97-120, stable: starts[C+1] (starts[C] = n) and
+ * the permutation perm[n] (slot -> input index, ascending index inside a
+ * cell). All pointers are device memory; keys may be null. `stream` is a
+ * cudaStream_t (null: the legacy default stream). Asynchronous. */
+int32_t fluid_grid_build(const float *pos4, uint32_t n, const FluidGrid *grid, uint32_t *keys,
+                         uint32_t *starts, uint32_t *perm, void *workspace, uint64_t ws_bytes,
+                         void *stream);
+
+/* The same from and to host memory (allocates, copies, synchronises). */
+int32_t fluid_grid_build_host(const float *pos4, uint32_t n, const FluidGrid *grid,
+                              uint32_t *starts, uint32_t *perm);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

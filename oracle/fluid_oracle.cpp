@@ -10,7 +10,7 @@
 //   - dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z; mix(a, b, t) = a*(1-t) + b*t;
 //   - exp inside a kernel is or_exp below (a fixed Cody-Waite + Taylor
 //     evaluation); exp of a per-substep constant is libm expf on the host;
-//   - every global sum is exact: per-particle FP64 terms in 2^-32 fixed point,
+//   - every global sum is exact: per-particle FP64 terms in 2^-28 fixed point,
 //     summed as 64-bit integers, so the total does not depend on order.
 #include "fluid_oracle.h"
 
@@ -102,11 +102,13 @@ inline uint32_t pcg(uint32_t x) {  // sim_tracers.wgsl:54-58
     return (h >> 22u) ^ h;
 }
 
-// 64-bit fixed-point accumulation of non-negative FP64 terms (2^-32 units).
+// 64-bit fixed-point accumulation of non-negative FP64 terms: 2^-28 units,
+// each term capped at 16, so no sum over 2^32 particles can wrap.
+constexpr double kFixedScale = 268435456.0;
 inline int64_t fx(double term) {
     if (!(term > 0.0)) return 0;
-    if (term > 1.0e3) term = 1.0e3;
-    return (int64_t)std::llrint(term * 4294967296.0);
+    if (term > 16.0) term = 16.0;
+    return (int64_t)std::llrint(term * kFixedScale);
 }
 
 }  // namespace
@@ -1107,7 +1109,7 @@ void or_sim_substep(OrSim *s, const OrStep *st, uint32_t div_iters, uint32_t den
 // one measured after its last apply.
 void or_sim_substep_tol(OrSim *s, const OrStep *st, float div_tol, float den_tol,
                         uint32_t max_iters, uint32_t out_iters[2], double out_res[2]) {
-    const double scale = 1.0 / 4294967296.0 / (double)s->n;
+    const double scale = 1.0 / kFixedScale / (double)s->n;
     rebuild(s);
     int64_t acc = density_div(s, st->dt);
     out_iters[0] = out_iters[1] = 0;
@@ -1150,7 +1152,7 @@ void or_sim_stats(OrSim *s, float out[14]) {
         lo = fminw(lo, s->density[i]);
         hi = fmaxw(hi, s->density[i]);
     }
-    out[0] = (float)((double)sum / 4294967296.0 / (double)n);
+    out[0] = (float)((double)sum / kFixedScale / (double)n);
     out[1] = fmaxw(m, 0.0f);
     out[2] = lo;
     out[3] = hi;

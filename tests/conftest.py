@@ -18,3 +18,20 @@ def orc():
     from oracle import oracle
     oracle.lib()
     return oracle
+
+
+def _load_product():
+    import importlib.util
+    path = os.path.join(ROOT, "fluid-simulation-app_b200", "fluidcu.py")
+    spec = importlib.util.spec_from_file_location("fluidcu", path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["fluidcu"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="session")
+def fcu():
+    mod = _load_product()
+    mod.lib()
+    return mod
