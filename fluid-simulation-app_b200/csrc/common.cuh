@@ -8,6 +8,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <stddef.h>
 #include <stdint.h>
 
 #include "../../include/fluid_cu.h"
@@ -56,17 +57,22 @@ struct DevStep {
 constexpr int kAccSlots = 128;
 constexpr uint32_t kMaxIters = kAccSlots - 2;
 
-// Per-substep solver counters the host reads back.
+// Per-substep solver counters the host reads back (the head, up to
+// acc_div, is what a statistics read copies), then the accumulators.
 struct DevSolve {
-    unsigned long long acc_div[kAccSlots];  // fixed-point residual sums (2^-28)
-    unsigned long long acc_den[kAccSlots];
     double div_res, den_res;
     uint32_t div_iters, den_iters;
     uint32_t clamp_count, nbr_over;  // cumulative
     uint32_t error;
     uint32_t cursor;  // step ring read position
     unsigned long long substeps;
+    unsigned long long total_div_iters;  // cumulative applies since create
+    unsigned long long total_den_iters;
+    unsigned long long acc_div[kAccSlots];  // fixed-point residual sums (2^-28)
+    unsigned long long acc_den[kAccSlots];
 };
+constexpr size_t kSolveHeadBytes = 64;
+static_assert(offsetof(DevSolve, acc_div) == kSolveHeadBytes, "DevSolve head");
 
 struct F3 {
     float x, y, z;

@@ -104,6 +104,8 @@ struct FluidSim {
     uint64_t h_cursor = 0, synced_cursor = 0;
     std::map<std::pair<uint32_t, uint32_t>, cudaGraphExec_t> graphs;
     cudaGraphExec_t density_graph = nullptr;
+    cudaGraphExec_t tol_graph = nullptr;
+    cudaStream_t side = nullptr;  // captures the loop bodies
     std::vector<void *> allocs;
     float stats_host[14]{};
     uint32_t last_frame_substeps = 0;
@@ -278,7 +280,7 @@ GridGeom geom_of(const DevParams &P) {
 template <class Mark>
 cudaError_t enqueue_substep(FluidSim *s, cudaStream_t st, uint32_t div_iters, uint32_t den_iters,
                             bool density_only, Mark mark) {
-    cudaError_t e = cudaMemsetAsync(s->solve, 0, 2 * kAccSlots * sizeof(unsigned long long), st);
+    cudaError_t e = cudaMemsetAsync(s->solve->acc_div, 0, 2 * kAccSlots * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     e = grid_build_enqueue(st, s->b.pos, s->n, geom_of(s->P), s->b.keys, s->b.starts, s->b.perm, s->gw,
                            true, s->ring, s->cur, s->solve, kRing);
@@ -339,6 +341,98 @@ int32_t graph_for(FluidSim *s, uint32_t div_iters, uint32_t den_iters, cudaGraph
     if (rc == FLUID_OK) s->graphs[key] = *out;
     return rc;
 }
+
+// Adds a WHILE node after the capture's current frontier and makes it the
+// frontier; returns its body graph.
+int32_t add_while(cudaStream_t st, cudaGraph_t g, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+    cudaStreamCaptureStatus status;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    CK(cudaStreamGetCaptureInfo(st, &status, nullptr, nullptr, &deps, &nd));
+    cudaGraphNodeParams p = {cudaGraphNodeTypeConditional};
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g, deps, nd, &p));
+    *body = p.conditional.phGraph_out[0];
+    CK(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return FLUID_OK;
+}
+
+// The tolerance substep: the same sweeps as the fixed schedule, with the
+// divergence and density iterations as device-side loops (graph WHILE
+// nodes) that a one-thread kernel continues or stops from the exact FP64
+// residual, so no iteration waits on the host.
+int32_t capture_tolerance(FluidSim *s, cudaGraphExec_t *out) {
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    cudaGraphConditionalHandle hdiv, hden;
+    CK(cudaGraphConditionalHandleCreate(&hdiv, g, 0, 0));
+    CK(cudaGraphConditionalHandleCreate(&hden, g, 0, 0));
+    const FluidSimConfig &c = s->cfg;
+    cudaStream_t st = s->stream;
+    cudaGraph_t bdiv = nullptr, bden = nullptr;
+    CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int32_t rc = FLUID_OK;
+    cudaError_t e = cudaMemsetAsync(s->solve->acc_div, 0, 2 * kAccSlots * sizeof(unsigned long long), st);
+    if (e == cudaSuccess)
+        e = grid_build_enqueue(st, s->b.pos, s->n, geom_of(s->P), s->b.keys, s->b.starts, s->b.perm, s->gw,
+                               true, s->ring, s->cur, s->solve, kRing);
+    if (e == cudaSuccess) {
+        launch_gather(st, s->b, s->n);
+        launch_density_div(st, s->P, s->b, s->cur, s->solve, &s->solve->acc_div[0]);
+        launch_tol_finish(st, s->solve, s->n, 0, 1, c.div_tol, c.max_iters, hdiv);
+        rc = add_while(st, g, hdiv, &bdiv);
+    }
+    if (e == cudaSuccess && rc == FLUID_OK) {
+        launch_forces_eval(st, s->P, s->b);
+        launch_forces_apply(st, s->P, s->b, s->cur);
+        launch_den_kappa(st, s->P, s->b, s->cur, &s->solve->acc_den[0]);
+        launch_tol_finish(st, s->solve, s->n, 1, 1, c.den_tol, c.max_iters, hden);
+        rc = add_while(st, g, hden, &bden);
+    }
+    if (e == cudaSuccess && rc == FLUID_OK)
+        launch_integrate(st, s->P, s->b, s->cur, s->solve, -1, -1, 0, 0);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    cudaGraph_t g2 = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(st, &g2);
+    if (rc != FLUID_OK || e != cudaSuccess || e2 != cudaSuccess) {
+        cudaGraphDestroy(g);
+        if (rc != FLUID_OK) return rc;
+        return fail(FLUID_ERR_CUDA, std::string("tolerance capture: ") +
+                                        cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    // loop bodies
+    CK(cudaStreamBeginCaptureToGraph(s->side, bdiv, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launch_apply(s->side, s->P, s->b, s->cur, false);
+    launch_div_kappa(s->side, s->P, s->b, s->cur, &s->solve->acc_div[0]);
+    launch_tol_finish(s->side, s->solve, s->n, 0, 0, c.div_tol, c.max_iters, hdiv);
+    CK(cudaStreamEndCapture(s->side, &bdiv));
+    CK(cudaStreamBeginCaptureToGraph(s->side, bden, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    launch_apply(s->side, s->P, s->b, s->cur, true);
+    launch_den_kappa(s->side, s->P, s->b, s->cur, &s->solve->acc_den[0]);
+    launch_tol_finish(s->side, s->solve, s->n, 1, 0, c.den_tol, c.max_iters, hden);
+    CK(cudaStreamEndCapture(s->side, &bden));
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(FLUID_ERR_CUDA, std::string("instantiate: ") + cudaGetErrorString(e));
+    return FLUID_OK;
+}
+
+// The graph of one substep in the handle's schedule.
+int32_t substep_graph(FluidSim *s, uint32_t den_fixed, cudaGraphExec_t *out) {
+    if (s->cfg.solve == FLUID_SOLVE_TOLERANCE) {
+        if (!s->tol_graph) {
+            int32_t rc = capture_tolerance(s, &s->tol_graph);
+            if (rc != FLUID_OK) return rc;
+        }
+        *out = s->tol_graph;
+        return FLUID_OK;
+    }
+    return graph_for(s, s->cfg.div_iters, den_fixed, out);
+}
+
 
 // Places `count` Step blocks in the ring (pinned mirror, then one or two
 // copies) for the next `count` substeps.
@@ -451,11 +545,13 @@ void fluid_sim_destroy(FluidSim *s) {
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
     if (s->density_graph) cudaGraphExecDestroy(s->density_graph);
+    if (s->tol_graph) cudaGraphExecDestroy(s->tol_graph);
     for (void *p : s->allocs) cudaFree(p);
     if (s->grid_ws) cudaFree(s->grid_ws);
     if (s->h_ring) cudaFreeHost(s->h_ring);
     if (s->h_stats_stale) cudaFreeHost(s->h_stats_stale);
     if (s->stats_ready) cudaEventDestroy(s->stats_ready);
+    if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
 }
@@ -547,8 +643,9 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
         CK(cudaMemcpy(b.tracers, tr.data(), 8ull * s->ntr, cudaMemcpyHostToDevice));
     }
     CK(cudaDeviceSynchronize());
+    CK(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
     cudaGraphExec_t g;
-    int32_t rc = graph_for(s, cfg->div_iters, cfg->den_iters, &g);
+    int32_t rc = substep_graph(s, cfg->den_iters, &g);
     if (rc != FLUID_OK) return rc;
     return FLUID_OK;
 }
@@ -600,7 +697,7 @@ int32_t fluid_sim_run(FluidSim *s, const FluidStep *steps, uint32_t count) {
                 }
                 g = s->density_graph;
             } else {
-                rc = graph_for(s, s->cfg.div_iters, s->cfg.den_iters, &g);
+                rc = substep_graph(s, s->cfg.den_iters, &g);
                 if (rc != FLUID_OK) return rc;
             }
             CK(cudaGraphLaunch(g, s->stream));
@@ -660,7 +757,7 @@ int32_t fluid_sim_stats(FluidSim *s, FluidSimStats *out) {
     float st[16];
     DevSolve sv;
     CK(cudaMemcpy(st, s->b.stats, sizeof st, cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&sv, s->solve, sizeof sv, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&sv, s->solve, kSolveHeadBytes, cudaMemcpyDeviceToHost));
     std::memset(out, 0, sizeof *out);
     out->compression_avg = st[0];
     out->compression_max = st[1];
@@ -681,6 +778,8 @@ int32_t fluid_sim_stats(FluidSim *s, FluidSimStats *out) {
     out->div_residual = sv.div_res;
     out->den_residual = sv.den_res;
     out->substeps = sv.substeps;
+    out->total_div_iters = sv.total_div_iters;
+    out->total_den_iters = sv.total_den_iters;
     out->substeps_last_frame = s->last_frame_substeps;
     out->error = sv.error ? FLUID_ERR_TIMEOUT : FLUID_OK;
     bool finite = true;
@@ -780,7 +879,7 @@ int32_t fluid_sim_read_field(FluidSim *s, int32_t field, void *out, uint64_t byt
     case FLUID_FIELD_COUNTERS: {
         if (bytes < 8) return fail(FLUID_ERR_ARG, "buffer too small");
         DevSolve sv;
-        CK(cudaMemcpy(&sv, s->solve, sizeof sv, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(&sv, s->solve, kSolveHeadBytes, cudaMemcpyDeviceToHost));
         ((uint32_t *)out)[0] = sv.clamp_count;
         ((uint32_t *)out)[1] = sv.nbr_over;
         return FLUID_OK;
@@ -882,7 +981,7 @@ int32_t fluid_sim_frame(FluidSim *s, FluidVec3 force, FluidVec3 omega, FluidVec3
     int32_t rc = upload_steps(s, steps.data(), n);
     if (rc != FLUID_OK) return rc;
     cudaGraphExec_t g;
-    rc = graph_for(s, s->cfg.div_iters, refine_passes(dt_sub), &g);
+    rc = substep_graph(s, refine_passes(dt_sub), &g);
     if (rc != FLUID_OK) return rc;
     for (uint32_t k = 0; k < n; ++k) CK(cudaGraphLaunch(g, s->stream));
     launch_stats(s->stream, s->P, s->b, s->solve);

@@ -533,22 +533,33 @@ __global__ void __launch_bounds__(256) k_integrate(DevParams P, SimBufs b,
                 den_slot >= 0 ? (double)solve->acc_den[den_slot] / kFixedScale / (double)n : 0.0;
             solve->div_iters = (uint32_t)div_iters;
             solve->den_iters = (uint32_t)den_iters;
+            solve->total_div_iters += (unsigned long long)div_iters;
+            solve->total_den_iters += (unsigned long long)den_iters;
         }
     }
 }
 
-// Records the residual of slot `slot` (fixed schedule) or of slot 0 and
-// clears it (tolerance loop).
-__global__ void k_finish_residual(DevSolve *solve, uint32_t n, int which, int count_iter,
-                                  int reset_iters) {
-    unsigned long long *acc = which == 0 ? solve->acc_div : solve->acc_den;
-    const double res = (double)acc[0] / kFixedScale / (double)n;
-    acc[0] = 0ull;
+// The tolerance loop's bookkeeping (one thread): reads and clears the
+// residual accumulator of `which` (0 divergence, 1 density), counts the
+// iteration unless `first`, records the residual, and sets the graph's
+// loop condition: go on while under max_iters and the residual is above
+// tol (the divergence loop always makes its first apply, as the reference).
+__global__ void k_tol_finish(DevSolve *solve, uint32_t n, int which, int first, float tol,
+                             uint32_t max_iters, cudaGraphConditionalHandle handle) {
+    unsigned long long *acc = which == 0 ? &solve->acc_div[0] : &solve->acc_den[0];
+    const double res = (double)*acc / kFixedScale / (double)n;
+    *acc = 0ull;
     uint32_t *iters = which == 0 ? &solve->div_iters : &solve->den_iters;
-    if (reset_iters) *iters = 0;
-    if (count_iter) *iters += 1;
+    const uint32_t it = first ? 0u : *iters + 1u;
+    *iters = it;
+    if (!first) {
+        if (which == 0) solve->total_div_iters += 1ull;
+        else solve->total_den_iters += 1ull;
+    }
     if (which == 0) solve->div_res = res;
     else solve->den_res = res;
+    const bool go = it < max_iters && (res > (double)tol || (which == 0 && it < 1u));
+    cudaGraphSetConditional(handle, go ? 1u : 0u);
 }
 
 // ---- reduce_stats (sim_solve.wgsl:800-874) ---------------------------------
@@ -795,9 +806,9 @@ void launch_integrate(cudaStream_t s, const DevParams &P, const SimBufs &b, cons
     k_integrate<<<blocks_for(P.count, 256), 256, 0, s>>>(P, b, st, solve, div_slot, den_slot,
                                                          div_iters, den_iters);
 }
-void launch_finish_residual(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int count_iter,
-                            int reset_iters) {
-    k_finish_residual<<<1, 1, 0, s>>>(solve, n, which, count_iter, reset_iters);
+void launch_tol_finish(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int first, float tol,
+                       uint32_t max_iters, cudaGraphConditionalHandle handle) {
+    k_tol_finish<<<1, 1, 0, s>>>(solve, n, which, first, tol, max_iters, handle);
 }
 void launch_stats(cudaStream_t s, const DevParams &P, const SimBufs &b, DevSolve *solve) {
     uint32_t blocks = blocks_for(P.count, kStatsThreads);

@@ -48,11 +48,10 @@ void launch_den_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, cons
                       unsigned long long *acc);
 void launch_integrate(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
                       DevSolve *solve, int div_slot, int den_slot, int div_iters, int den_iters);
-// Residual bookkeeping after a sweep that accumulated one: which = 0
-// divergence, 1 density. Records the residual, bumps the iteration count
-// when `count_iter`, clears the accumulator.
-void launch_finish_residual(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int count_iter,
-                            int reset_iters);
+// The tolerance loop's step after a prediction sweep: records the residual
+// of `which` (0 divergence, 1 density), counts the iteration, sets `handle`.
+void launch_tol_finish(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int first, float tol,
+                       uint32_t max_iters, cudaGraphConditionalHandle handle);
 void launch_stats(cudaStream_t s, const DevParams &P, const SimBufs &b, DevSolve *solve);
 void launch_splat(cudaStream_t s, const DevParams &P, const SimBufs &b);
 void launch_resolve(cudaStream_t s, const DevParams &P, const SimBufs &b);

@@ -64,7 +64,8 @@ class FluidSimStats(C.Structure):
                 ("v_min", C.c_float), ("accel_min", C.c_float), ("accel_max", C.c_float),
                 ("div_iters", C.c_uint32), ("den_iters", C.c_uint32),
                 ("div_residual", C.c_double), ("den_residual", C.c_double),
-                ("substeps", C.c_uint64), ("substeps_last_frame", C.c_uint32),
+                ("substeps", C.c_uint64), ("total_div_iters", C.c_uint64),
+                ("total_den_iters", C.c_uint64), ("substeps_last_frame", C.c_uint32),
                 ("error", C.c_int32)]
 
     def as_reference_block(self):

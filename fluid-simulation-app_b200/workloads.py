@@ -1,0 +1,122 @@
+"""The synthetic workloads the DFSPH step is measured and tested on.
+
+No public benchmark or dataset exists for this path; every input is a seeded
+lattice or point cloud built here with the shapes, sizes and distributions
+of the five workloads:
+
+  dam_break_16k   32x16x32 lattice (16,384), unit box, spacing 0.01, h = 2r,
+                  rho0 1000, XSPH 0.01, gravity (0, -9.81, 0), dt 1/120
+  tilt_1m         128x64x128 lattice (1,048,576), box 1.28 x 0.64 x 1.28,
+                  spacing 0.005, gravity rotated by a seeded tilt sequence,
+                  4,096 tracers, dt 1/120
+  grid_16m        16,777,216 positions in a 256^3-cell box (three
+                  distributions), grid build alone
+  batched_256     256 boxes, 4,096..65,536 particles each (log-uniform)
+  adjoint_64k     64x16x64 lattice (65,536), 120 steps
+
+Reading of "h = 4r": the support radius 2h of the cubic spline is 4r, so the
+kernel h equals the spacing 2r (h_ratio 1.0) and the grid cell (= support)
+is 4r, which makes the 27-cell stencil exact. Lattice jitter is +-0.01 r =
++-0.005 spacing from a splitmix64 stream.
+
+The tilt: gravity (0, -9.81, 0) rotated about x by theta_x(t) and then about
+z by theta_z(t); each theta is a sum of three sinusoids a_k sin(2 pi f_k t +
+phi_k) with a_k in [35/6, 35/3] degrees (so sum a_k <= 35 degrees),
+f_k ~ U[0.2, 2] Hz and phi_k ~ U[0, 2 pi), all drawn from numpy's PCG64
+seeded with the workload seed. This is the construction of the reference's
+TILT film pose (crates/fluid-core/examples/film.rs:121-130), made seeded.
+"""
+import math
+
+import numpy as np
+
+G = 9.81
+F32 = np.float32
+
+
+def tilt_schedule(seed, steps, dt):
+    """Body force per step, float32 (steps, 3)."""
+    rng = np.random.default_rng(seed)
+    amp = np.radians(rng.uniform(35.0 / 6.0, 35.0 / 3.0, (2, 3)))
+    freq = rng.uniform(0.2, 2.0, (2, 3))
+    phase = rng.uniform(0.0, 2.0 * math.pi, (2, 3))
+    t = np.arange(steps, dtype=np.float64)[:, None] * dt
+    tx = np.sum(amp[0] * np.sin(2 * math.pi * freq[0] * t + phase[0]), axis=1)
+    tz = np.sum(amp[1] * np.sin(2 * math.pi * freq[1] * t + phase[1]), axis=1)
+    g = np.array([0.0, -G, 0.0])
+    # R = Rz(tz) Rx(tx) g
+    gx = np.zeros((steps, 3))
+    y = g[1] * np.cos(tx)
+    z = g[1] * np.sin(tx)
+    gx[:, 0] = -y * np.sin(tz)
+    gx[:, 1] = y * np.cos(tz)
+    gx[:, 2] = z
+    return gx.astype(np.float32)
+
+
+def v_clamp(spacing, dt):
+    """The CFL speed of render.rs:3171: 0.4 spacing / dt, in f32."""
+    return float(F32(0.4) * F32(spacing) / F32(dt))
+
+
+def box_config(fcu, lattice, box_hi, spacing, tracers=0, seed=1, xsph=0.01, solve=None,
+               div_tol=0.01, den_tol=0.001, max_iters=100, **kw):
+    cfg = dict(geometry=fcu.GEOMETRY_BOX, box_lo=(0.0, 0.0, 0.0), box_hi=box_hi, spacing=spacing,
+               h_ratio=1.0, rest_density=1000.0, seeding=fcu.SEED_BLOCK, block=lattice,
+               jitter=0.005, seed=seed, xsph_blend=xsph, tracers=tracers,
+               solve=fcu.SOLVE_TOLERANCE if solve is None else solve, div_tol=div_tol,
+               den_tol=den_tol, max_iters=max_iters)
+    cfg.update(kw)
+    return fcu.default_config(**cfg)
+
+
+WORKLOADS = {
+    "dam_break_16k": dict(lattice=(32, 16, 32), box_hi=(1.0, 1.0, 1.0), spacing=0.01,
+                          tracers=0, steps=240, tilt=False),
+    "tilt_1m": dict(lattice=(128, 64, 128), box_hi=(1.28, 0.64, 1.28), spacing=0.005,
+                    tracers=4096, steps=600, tilt=True),
+    "adjoint_64k": dict(lattice=(64, 16, 64), box_hi=(1.28, 0.64, 1.28), spacing=0.005,
+                        tracers=0, steps=120, tilt=True),
+}
+
+
+def make_config(fcu, name, **over):
+    w = WORKLOADS[name]
+    kw = dict(tracers=w["tracers"])
+    kw.update(over)
+    return box_config(fcu, w["lattice"], w["box_hi"], w["spacing"], **kw)
+
+
+def steps_for(fcu, name, steps, dt=1.0 / 120.0, seed=1, start=0):
+    """Step blocks for `steps` substeps of workload `name` from step `start`."""
+    w = WORKLOADS[name]
+    dt32 = float(F32(dt))
+    vc = v_clamp(w["spacing"], dt32)
+    if w["tilt"]:
+        forces = tilt_schedule(seed, start + steps, dt)[start:]
+    else:
+        forces = np.tile(np.array([[0.0, -G, 0.0]], np.float32), (steps, 1))
+    return [fcu.make_step(force=tuple(float(v) for v in f), dt=dt32, v_clamp=vc, seed=start + k)
+            for k, f in enumerate(forces)]
+
+
+def grid_positions(kind, n, side, seed):
+    """The 16.7M-position grid workload's three distributions, float4."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros((n, 4), np.float32)
+    if kind == "uniform":
+        p[:, :3] = rng.uniform(0, side, (n, 3))
+    elif kind == "packed":
+        k = int(n * 0.9)
+        p[:k, :3] = rng.uniform(0, side, (k, 3))
+        p[:k, 1] = rng.uniform(0, side * 0.1, k)
+        p[k:, :3] = rng.uniform(0, side, (n - k, 3))
+    elif kind == "gaussian":
+        centres = rng.uniform(side / 8, side * 7 / 8, (8, 3))
+        per = n // 8
+        for c in range(8):
+            m = per if c < 7 else n - 7 * per
+            p[c * per:c * per + m, :3] = centres[c] + rng.normal(0, 4.0, (m, 3))
+    else:
+        raise ValueError(kind)
+    return p

@@ -139,6 +139,8 @@ typedef struct FluidSimStats {
     double div_residual;   /* last substep, after its last divergence apply */
     double den_residual;   /* last substep, after its last density apply */
     uint64_t substeps;     /* substeps run since create */
+    uint64_t total_div_iters; /* divergence applies since create */
+    uint64_t total_den_iters; /* density applies since create, warm starts excluded */
     uint32_t substeps_last_frame;
     int32_t error;         /* sticky device error (FLUID_ERR_*) */
 } FluidSimStats;

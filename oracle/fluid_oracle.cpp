@@ -1109,30 +1109,31 @@ void or_sim_substep(OrSim *s, const OrStep *st, uint32_t div_iters, uint32_t den
 // one measured after its last apply.
 void or_sim_substep_tol(OrSim *s, const OrStep *st, float div_tol, float den_tol,
                         uint32_t max_iters, uint32_t out_iters[2], double out_res[2]) {
-    const double scale = 1.0 / kFixedScale / (double)s->n;
+    const double n = (double)s->n;
+    auto mean = [n](int64_t acc) { return (double)acc / kFixedScale / n; };
     rebuild(s);
     int64_t acc = density_div(s, st->dt);
     out_iters[0] = out_iters[1] = 0;
-    out_res[0] = (double)acc * scale;
+    out_res[0] = mean(acc);
     out_res[1] = 0.0;
     if (st->dt == 0.0f) return;
     uint32_t it = 0;
-    double res = (double)acc * scale;
+    double res = mean(acc);
     while (it < max_iters && (it < 1 || res > (double)div_tol)) {
         apply_kappa(s, st->dt, false);
         it++;
-        res = (double)div_kappa(s, st->dt) * scale;
+        res = mean(div_kappa(s, st->dt));
     }
     out_iters[0] = it;
     out_res[0] = res;
     forces_eval(s);
     forces_den_apply(s, *st, step_xsph_blend(s->p, st->dt));
-    res = (double)den_kappa(s, st->dt) * scale;
+    res = mean(den_kappa(s, st->dt));
     it = 0;
     while (it < max_iters && res > (double)den_tol) {
         apply_kappa(s, st->dt, true);
         it++;
-        res = (double)den_kappa(s, st->dt) * scale;
+        res = mean(den_kappa(s, st->dt));
     }
     out_iters[1] = it;
     out_res[1] = res;

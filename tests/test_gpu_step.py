@@ -216,3 +216,28 @@ def test_the_step_is_bit_reproducible(fcu):
         outs.append(sim.state())
     for k in outs[0]:
         assert_same_bits(outs[0][k], outs[1][k], k)
+
+
+# The tolerance schedule: device-side loops stop on the exact FP64 residual,
+# so iteration counts, residuals and states all match the oracle's loop.
+@pytest.mark.parametrize("tols", [(0.01, 0.001), (0.002, 0.0002)])
+def test_the_tolerance_schedule_matches_the_oracle(fcu, orc, tols):
+    div_tol, den_tol = tols
+    cfg = dict(geometry=fcu.GEOMETRY_BOX, box_lo=(0, 0, 0), box_hi=(0.4, 0.4, 0.4), spacing=0.01,
+               h_ratio=1.0, rest_density=1000.0, seeding=fcu.SEED_BLOCK, block=(16, 12, 16),
+               jitter=0.005, seed=3, xsph_blend=0.01, solve=fcu.SOLVE_TOLERANCE, div_tol=div_tol,
+               den_tol=den_tol, max_iters=100)
+    sim, o = pair(fcu, orc, **cfg)
+    dt = float(F32(1.0 / 120.0))
+    s_g, s_o = step_pair(fcu, orc, force=(0.5, -9.81, 0.2), dt=dt, v_clamp=v_clamp(0.01, dt))
+    seen = set()
+    for k in range(40):
+        sim.step(s_g)
+        iters, res = o.substep_tol(s_o, div_tol, den_tol, 100)
+        st = sim.stats()
+        assert (st.div_iters, st.den_iters) == (int(iters[0]), int(iters[1])), k
+        assert st.div_residual == res[0] and st.den_residual == res[1], k
+        assert st.den_residual <= den_tol or st.den_iters == 100
+        seen.add(int(iters[1]))
+    same_state(sim, o, "tolerance")
+    assert len(seen) > 1, "the iteration count never varied"
