@@ -1,0 +1,399 @@
+#!/usr/bin/env python
+"""Throughput of the B200 DFSPH step on the 1M-particle tilt workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+A bench step is one 1/120 s frame of the tilt_1m workload (1,048,576
+particles, 128x64x128 lattice in a 1.28 x 0.64 x 1.28 m box, 4,096 tracers,
+seeded tilt), advanced the way Renderer::frame does it (render.rs:3021-3229):
+substeps_for picks the substeps, each substep runs the tolerance solve (1 %
+divergence, 0.1 % density, at most 100 iterations), then reduce_stats and one
+tracer pass. The metric counts executed substeps: particle-steps/s.
+
+value: K frames launched back to back on the sim's stream, timed with CUDA
+events; the state lives in HBM (working set ~0.5 GB, past the 126 MB L2, so
+no flush is needed). e2e: the same frames through the C ABI with a stats
+read back to host memory after every frame, wall-clocked. roofline: the
+dominant kernel, timed kernel by kernel with CUDA events on the sim's
+stream. cpu_baseline: the CPU oracle on this host's cores over a bounded
+sample (one substep of the same state). N > 1: one independent replica per
+GPU (a single box does not shard), max over ranks.
+"""
+import argparse
+import ctypes as C
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "fluid-simulation-app_b200")
+WORKLOAD = "tilt_1m"
+METRIC = "particle-steps/s at 0.1% density error: plain vs batched vs adjoint, 1×B200"
+UNIT = "particle-steps/s"
+
+# Algorithmic bytes per particle of each substep kernel: the particle's own
+# records it must read and write once (neighbour reads are cache hits in
+# cell order and not counted). keys+count 20, reorder 116, density 44,
+# divergence kappa 28 / apply 36, forces 84 / 92, density kappa 36 / apply
+# 36, integrate 120.
+ALGO_BYTES = {"grid": 20.0, "gather": 116.0, "density_div": 44.0, "div_kappa": 28.0,
+              "div_apply": 36.0, "forces_eval": 84.0, "forces_den_apply": 92.0,
+              "den_kappa": 36.0, "den_apply": 36.0, "integrate": 120.0}
+# DRAM bytes per particle per launch, from one ncu capture of each kernel on
+# a 131,072-particle case of the same workload (profiles/; traffic grows in
+# proportion to the particles). None until captured.
+NCU_TRAFFIC_PER_PARTICLE = {}
+
+
+def load(name, path):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while timing."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms",
+                 "100", "-i", str(self.device)], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.thread.join(timeout=2)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cuda_arm(args):
+    import torch
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    fcu = load("fluidcu", os.path.join(PKG, "fluidcu.py"))
+    wl = load("workloads", os.path.join(PKG, "workloads.py"))
+    w = wl.WORKLOADS[WORKLOAD]
+    frames = args.warmup + args.steps
+    forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
+    dt = float(np.float32(1.0 / 120.0))
+
+    def frame(sim, k):
+        f = forces[k]
+        sim.frame((float(f[0]), float(f[1]), float(f[2])), dt, substeps=0, cap=16, seed=k)
+
+    cfg = wl.make_config(fcu, WORKLOAD, device=local)
+    sim = fcu.Sim(cfg)
+    stream = torch.cuda.ExternalStream(sim.stream())
+    for k in range(args.warmup):
+        frame(sim, k)
+    sim.sync()
+    before = sim.stats()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clocks:
+        e0.record(stream)
+        for k in range(args.warmup, frames):
+            frame(sim, k)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sim.sync()
+    after = sim.stats()
+    substeps = int(after.substeps - before.substeps)
+    div_it = int(after.total_div_iters - before.total_div_iters)
+    den_it = int(after.total_den_iters - before.total_den_iters)
+    n = sim.n
+    if world > 1:
+        t = torch.tensor([ms, substeps], dtype=torch.float64, device="cuda")
+        tmax = t.clone()
+        torch.distributed.all_reduce(tmax[:1], op=torch.distributed.ReduceOp.MAX)
+        tot = t.clone()
+        torch.distributed.all_reduce(tot[1:], op=torch.distributed.ReduceOp.SUM)
+        ms_max, all_substeps = float(tmax[0]), float(tot[1])
+    else:
+        ms_max, all_substeps = ms, float(substeps)
+    value = n * all_substeps / (ms_max / 1000.0)
+
+    # kernel launches inside the timed region: per substep the grid build
+    # (keys, scan, 3 per digit pass), gather, density_div and its residual
+    # step, forces pair, first density prediction and its residual step,
+    # integrate; 3 per loop iteration; per frame stats (2) and tracers (3).
+    passes = 1
+    cells = sim.cells
+    while (cells - 1) >> (8 * passes):
+        passes += 1
+    fixed = 2 + 3 * passes + 1 + 2 + 4 + 1
+    launches = fixed * substeps + 3 * (div_it + den_it) + 5 * args.steps
+
+    # e2e: a fresh replica, frames through the C ABI with a stats read back
+    # to host memory after every frame (the frame's result), wall-clocked.
+    # Per frame: the substeps' Step blocks up (160 B each), the stale-stats
+    # copy, the statistics and the solver counters down (64 B each).
+    if args.no_e2e:
+        return finish_without_e2e(args, sim, value, ms_max, substeps, launches, clocks, world, rank)
+    sim_e = fcu.Sim(wl.make_config(fcu, WORKLOAD, device=local))
+    for k in range(args.warmup):
+        frame(sim_e, k)
+        sim_e.stats()
+    if world > 1:
+        torch.distributed.barrier()
+    sb = sim_e.stats()
+    t0 = time.perf_counter()
+    for k in range(args.warmup, frames):
+        frame(sim_e, k)
+        sim_e.stats()
+    t1 = time.perf_counter()
+    se = sim_e.stats()
+    e2e_sub = int(se.substeps - sb.substeps)
+    e2e_s = t1 - t0
+    if world > 1:
+        t = torch.tensor([e2e_s, e2e_sub], dtype=torch.float64, device="cuda")
+        tm = t.clone()
+        torch.distributed.all_reduce(tm[:1], op=torch.distributed.ReduceOp.MAX)
+        ts = t.clone()
+        torch.distributed.all_reduce(ts[1:], op=torch.distributed.ReduceOp.SUM)
+        e2e_s, e2e_all = float(tm[0]), float(ts[1])
+    else:
+        e2e_all = float(e2e_sub)
+    e2e_value = n * e2e_all / e2e_s
+    sim_e.close()
+
+    # roofline: per-kernel CUDA-event times of a few substeps of this state
+    prof = {}
+    for k in range(8):
+        f = forces[(frames + k) % len(forces)]
+        vc = wl.v_clamp(w["spacing"], float(np.float32(dt) / np.float32(4.0)))
+        st = fcu.make_step(force=tuple(float(x) for x in f), dt=float(np.float32(dt) / np.float32(4.0)),
+                           v_clamp=vc)
+        for name, t in sim.profile_step(st):
+            prof.setdefault(name, []).append(t)
+    totals = {k: sum(v) for k, v in prof.items()}
+    dom = max((k for k in totals if k in ALGO_BYTES), key=lambda k: totals[k])
+    avg_ms = totals[dom] / len(prof[dom])
+    achieved = ALGO_BYTES[dom] * n / (avg_ms / 1000.0) / 1e9
+    peak, peak_kind = peaks()
+    traffic = NCU_TRAFFIC_PER_PARTICLE.get(dom)
+
+    # the CPU oracle on this host over one substep of the same state
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_sample(fcu, sim, dt)
+
+    sim.reduce_stats()
+    final = sim.stats()
+    sim.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "particles": n, "lattice": list(w["lattice"]),
+                       "box_m": list(w["box_hi"]), "spacing_m": w["spacing"], "h_ratio": 1.2,
+                       "tracers": w["tracers"], "frame_dt_s": dt,
+                       "step": "one DFSPH substep; substeps per 1/120 s frame by substeps_for",
+                       "substeps": substeps, "substeps_per_frame": substeps / args.steps,
+                       "solve": "tolerance div 1% / den 0.1%, cap 100, FP64 residuals",
+                       "mean_div_iters": div_it / max(substeps, 1),
+                       "mean_den_iters": den_it / max(substeps, 1),
+                       "parallelism": f"replicas x{world}" if world > 1 else "single box",
+                       "l2": "working set ~0.5 GB > 126 MB L2; no flush"},
+            "density_error": {"compression_avg": final.compression_avg,
+                              "compression_max": final.compression_max,
+                              "den_residual_last": final.den_residual,
+                              "clamps": final.clamp_count},
+            "particle_frames_per_s": n * world * args.steps / (ms_max / 1000.0),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 160 * e2e_sub / args.steps,
+                    "d2h_bytes_per_step": 64 + 64 + 64},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None if traffic is None else traffic * n,
+                         "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
+                         "kernel_ms": {k: sum(v) / len(v) for k, v in prof.items()}},
+            "cpu_baseline": cpu,
+            "clocks": clocks.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def finish_without_e2e(args, sim, value, ms_max, substeps, launches, clocks, world, rank):
+    sim.close()
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                          "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms_max / args.steps, "substeps": substeps,
+                          "gpu_launches": launches, "clocks": clocks.summary(),
+                          "note": "profiling run: no e2e, roofline or cpu baseline"}), flush=True)
+    if world > 1:
+        import torch
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def cpu_sample(fcu, sim, dt):
+    """The oracle over one substep of the GPU's current state, all cores."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+
+    p = orc.OrParams()
+    for name, _ in orc.OrParams._fields_:
+        v = getattr(sim.params, name)
+        if hasattr(v, "__len__"):
+            getattr(p, name)[:] = list(v)
+        else:
+            setattr(p, name, v)
+    o = orc.Sim(p, 0)
+    st = sim.state()
+    o.set_state(st["pos"], st["vel"], st["prev_vel"], st["prev_p"], st["temp"], st["id"])
+    dts = float(np.float32(dt) / np.float32(4.0))
+    step = orc.make_step(force=(0.0, -9.81, 0.0), dt=dts,
+                         v_clamp=float(np.float32(0.4) * np.float32(0.005) / np.float32(dts)))
+    t0 = time.perf_counter()
+    iters, _ = o.substep_tol(step, 0.01, 0.001, 100)
+    t = time.perf_counter() - t0
+    return {"value": sim.n / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"one substep of {sim.n} particles from the benchmark state "
+                      f"({int(iters[0])} div + {int(iters[1])} den iterations), {t:.1f} s"}
+
+
+def reference_arm(args):
+    """The CPU oracle as the reference implementation, all host threads."""
+    world, rank, local = dist_init()
+    if rank != 0:
+        return
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as orc
+    wl = load("workloads", os.path.join(PKG, "workloads.py"))
+    # A bounded sample per step: one substep of a 32x16x32 block of the same
+    # lattice, spacing and physics (the 1M box's corner), so K + W steps stay
+    # within minutes on the host.
+    lattice = [32, 16, 32]
+    spacing = 0.005
+    pos = orc.seed_block([0, 0, 0], spacing, lattice, 0.005, 1)
+    p = orc.params_box([0, 0, 0], [0.32, 0.16, 0.32], spacing, 1.2, 1000.0, len(pos))
+    p.xsph_blend = 0.01
+    o = orc.Sim(p, 0)
+    o.set_state(pos4=pos)
+    dt = float(np.float32(1.0 / 120.0) / np.float32(4.0))
+    forces = wl.tilt_schedule(1, args.warmup + args.steps, 1.0 / 120.0)
+    vc = float(np.float32(0.4) * np.float32(spacing) / np.float32(dt))
+
+    def one(k):
+        f = forces[k]
+        o.substep_tol(orc.make_step(force=tuple(float(x) for x in f), dt=dt, v_clamp=vc), 0.01,
+                      0.001, 100)
+
+    for k in range(args.warmup):
+        one(k)
+    t0 = time.perf_counter()
+    for k in range(args.warmup, args.warmup + args.steps):
+        one(k)
+    t = time.perf_counter() - t0
+    value = len(pos) * args.steps / t
+    cores = os.cpu_count()
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample": "32x16x32 block of the tilt_1m lattice"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"one substep of a {len(pos)}-particle block per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=120)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        cuda_arm(args)
+
+
+if __name__ == "__main__":
+    main()
