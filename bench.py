@@ -37,6 +37,7 @@ PKG = os.path.join(ROOT, "fluid-simulation-app_b200")
 WORKLOAD = "tilt_1m"
 METRIC = "particle-steps/s at 0.1% density error: plain vs batched vs adjoint, 1×B200"
 UNIT = "particle-steps/s"
+SUBSTEPS_PER_FRAME = 4
 
 # Algorithmic bytes per particle of each substep kernel: the particle's own
 # records it must read and write once (neighbour reads are cache hits in
@@ -145,9 +146,15 @@ def cuda_arm(args):
     forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
     dt = float(np.float32(1.0 / 120.0))
 
+    # Substeps per frame: substeps_for's floor at this spacing (render.rs:63-65,
+    # dt / (0.42 spacing) rounded up, four at 5 mm). Fixed rather than driven
+    # by the one-frame-stale v_max, so the device-timed and the end-to-end
+    # runs execute the same substeps on the same states.
+    sub = SUBSTEPS_PER_FRAME
+
     def frame(sim, k):
         f = forces[k]
-        sim.frame((float(f[0]), float(f[1]), float(f[2])), dt, substeps=0, cap=16, seed=k)
+        sim.frame((float(f[0]), float(f[1]), float(f[2])), dt, substeps=sub, cap=16, seed=k)
 
     cfg = wl.make_config(fcu, WORKLOAD, device=local)
     sim = fcu.Sim(cfg)
@@ -155,6 +162,8 @@ def cuda_arm(args):
     for k in range(args.warmup):
         frame(sim, k)
     sim.sync()
+    if args.profile_substeps:
+        return profile_only(args, fcu, wl, sim, forces, dt / sub, w)
     before = sim.stats()
     if world > 1:
         torch.distributed.barrier()
@@ -233,9 +242,8 @@ def cuda_arm(args):
     prof = {}
     for k in range(8):
         f = forces[(frames + k) % len(forces)]
-        vc = wl.v_clamp(w["spacing"], float(np.float32(dt) / np.float32(4.0)))
-        st = fcu.make_step(force=tuple(float(x) for x in f), dt=float(np.float32(dt) / np.float32(4.0)),
-                           v_clamp=vc)
+        dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
+        st = fcu.make_step(force=tuple(float(x) for x in f), dt=dts, v_clamp=wl.v_clamp(w["spacing"], dts))
         for name, t in sim.profile_step(st):
             prof.setdefault(name, []).append(t)
     totals = {k: sum(v) for k, v in prof.items()}
@@ -262,7 +270,7 @@ def cuda_arm(args):
             "config": {"workload": WORKLOAD, "particles": n, "lattice": list(w["lattice"]),
                        "box_m": list(w["box_hi"]), "spacing_m": w["spacing"], "h_ratio": 1.2,
                        "tracers": w["tracers"], "frame_dt_s": dt,
-                       "step": "one DFSPH substep; substeps per 1/120 s frame by substeps_for",
+                       "step": "one DFSPH substep; 4 per 1/120 s frame (substeps_for's floor at 5 mm)",
                        "substeps": substeps, "substeps_per_frame": substeps / args.steps,
                        "solve": "tolerance div 1% / den 0.1%, cap 100, FP64 residuals",
                        "mean_div_iters": div_it / max(substeps, 1),
@@ -289,6 +297,22 @@ def cuda_arm(args):
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def profile_only(args, fcu, wl, sim, forces, dt_sub, w):
+    """Substeps as direct kernel launches (visible to ncu), timed per kernel."""
+    prof = {}
+    vc = wl.v_clamp(w["spacing"], dt_sub)
+    for k in range(args.profile_substeps):
+        f = forces[k % len(forces)]
+        st = fcu.make_step(force=tuple(float(x) for x in f), dt=dt_sub, v_clamp=vc)
+        for name, t in sim.profile_step(st):
+            prof.setdefault(name, []).append(t)
+    sim.sync()
+    sim.close()
+    print(json.dumps({"profile_substeps": args.profile_substeps, "particles": int(sim.n),
+                      "kernel_ms": {k: sum(v) / len(v) for k, v in prof.items()},
+                      "launches": {k: len(v) for k, v in prof.items()}}), flush=True)
 
 
 def finish_without_e2e(args, sim, value, ms_max, substeps, launches, clocks, world, rank):
@@ -320,7 +344,7 @@ def cpu_sample(fcu, sim, dt):
     o = orc.Sim(p, 0)
     st = sim.state()
     o.set_state(st["pos"], st["vel"], st["prev_vel"], st["prev_p"], st["temp"], st["id"])
-    dts = float(np.float32(dt) / np.float32(4.0))
+    dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
     step = orc.make_step(force=(0.0, -9.81, 0.0), dt=dts,
                          v_clamp=float(np.float32(0.4) * np.float32(0.005) / np.float32(dts)))
     t0 = time.perf_counter()
@@ -386,6 +410,8 @@ def main():
     ap.add_argument("--impl", choices=["cuda", "reference"], default="cuda")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling runs)")
+    ap.add_argument("--profile-substeps", type=int, default=0,
+                    help="after the warm-up, run this many substeps as direct launches timed per kernel, then exit")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
