@@ -15,6 +15,23 @@
 
 #include "solve.cuh"
 
+// Neighbour batches of the list sweeps (see walk below): entries whose
+// records are loaded before any is used. Position + kappa records, position
+// + velocity records, and forces_eval's five records; FCU_MINB is the
+// minimum resident blocks per SM the sweeps are compiled for (0: none).
+#ifndef FCU_B_KD
+#define FCU_B_KD 8
+#endif
+#ifndef FCU_B_PV
+#define FCU_B_PV 8
+#endif
+#ifndef FCU_B_N5
+#define FCU_B_N5 4
+#endif
+#ifndef FCU_MINB
+#define FCU_MINB 0
+#endif
+
 namespace fcu {
 
 namespace {
@@ -193,6 +210,41 @@ __device__ __forceinline__ F3 pair_grad(const DevParams &P, F3 pos, float4 pj) {
     return grad_q(P, x, r, q);
 }
 
+// Walks particle i's neighbour list in list order, B entries at a time: the
+// B list words are loaded, then the B neighbours' records, and only then is
+// any of them used, so one batch's loads overlap instead of each neighbour
+// waiting on the round trip of the one before. The partial last batch loads
+// the particle's own record in its empty places and skips them. `use` sees
+// the neighbours in the same order as a plain loop, so every sum is the
+// same sum.
+template <int B, class T, class Load, class Use>
+__device__ __forceinline__ void walk(const uint32_t *__restrict__ nbr, uint32_t n, uint32_t i,
+                                     uint32_t cnt, Load load, Use use) {
+    for (uint32_t k = 0; k < cnt; k += B) {
+        uint32_t j[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) j[u] = (k + u < cnt) ? __ldg(&nbr[(size_t)(k + u) * n + i]) : i;
+        T v[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) v[u] = load(j[u]);
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (k + u < cnt) use(v[u]);
+    }
+}
+
+struct PosKd {
+    float4 p;
+    float kd;
+};
+struct PosVel {
+    float4 p, v;
+};
+struct Nbr5 {
+    float4 p, v;
+    float rho, temp, near;
+};
+
 // ---- gather into the working set (sim_grid.wgsl:52-63) -------------------
 __global__ void __launch_bounds__(256) k_gather(SimBufs b, uint32_t n) {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -225,8 +277,19 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimB
         const int by = (int)axis_cell(pos.y, P.box_min[1], P.cell, P.dims[1]);
         const int bz = (int)axis_cell(pos.z, P.box_min[2], P.cell, P.dims[2]);
         const int dx = (int)P.dims[0], dy = (int)P.dims[1], dz = (int)P.dims[2];
-        const int cx0 = bx > 0 ? bx - 1 : 0;
-        const int cx1 = bx + 1 < dx ? bx + 1 : dx - 1;
+        // Cell culling: a stencil cell whose nearest point lies beyond the
+        // support holds no neighbour, so skipping it changes neither the
+        // neighbour set nor its order. The distances to the own cell's faces
+        // are shrunk by a margin far above their rounding error (1e-3 cell
+        // plus 1e-6 |pos|, ~8 ulp of the coordinates), so a cell is culled
+        // only when every candidate in it would fail r2 < support^2.
+        const float margin = 1e-3f * P.cell + 1e-6f * (fabsf(pos.x) + fabsf(pos.y) + fabsf(pos.z));
+        const float fx = pos.x - (P.box_min[0] + (float)bx * P.cell);
+        const float fy = pos.y - (P.box_min[1] + (float)by * P.cell);
+        const float fz = pos.z - (P.box_min[2] + (float)bz * P.cell);
+        const float xl = fmaxf(fx - margin, 0.0f), xh = fmaxf(P.cell - fx - margin, 0.0f);
+        const float yl = fmaxf(fy - margin, 0.0f), yh = fmaxf(P.cell - fy - margin, 0.0f);
+        const float zl = fmaxf(fz - margin, 0.0f), zh = fmaxf(P.cell - fz - margin, 0.0f);
         float w_sum = P.sigma;
         float rho_near = 0.0f;
         F3 grad_sum = f3(0.f, 0.f, 0.f);
@@ -237,9 +300,14 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimB
         for (int oz = -1; oz <= 1; ++oz) {
             const int cz = bz + oz;
             if (cz < 0 || cz >= dz) continue;
+            const float dzp = oz < 0 ? zl * zl : (oz > 0 ? zh * zh : 0.0f);
             for (int oy = -1; oy <= 1; ++oy) {
                 const int cy = by + oy;
                 if (cy < 0 || cy >= dy) continue;
+                const float dperp = dzp + (oy < 0 ? yl * yl : (oy > 0 ? yh * yh : 0.0f));
+                if (dperp >= P.support_sq) continue;
+                const int cx0 = (bx > 0 && dperp + xl * xl < P.support_sq) ? bx - 1 : bx;
+                const int cx1 = (bx + 1 < dx && dperp + xh * xh < P.support_sq) ? bx + 1 : bx;
                 const uint32_t row = ((uint32_t)cz * (uint32_t)dy + (uint32_t)cy) * (uint32_t)dx;
                 const uint32_t s = __ldg(&b.starts[row + cx0]);
                 uint32_t e = __ldg(&b.starts[row + cx1 + 1]);
@@ -293,7 +361,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimB
 }
 
 // ---- divergence predictor for a later divergence iteration ---------------
-__global__ void __launch_bounds__(kSolveThreads) k_div_kappa(DevParams P, SimBufs b,
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(DevParams P, SimBufs b,
                                                              const DevStep *__restrict__ st,
                                                              unsigned long long *acc) {
     const uint32_t n = P.count;
@@ -305,11 +373,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_div_kappa(DevParams P, SimBuf
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
         float drho = 0.0f;
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
-            const F3 e = pair_grad(P, pos, __ldg(&b.wpos[j]));
-            drho += dot(vel - xyz(__ldg(&b.wvel[j])), e);
-        }
+        walk<FCU_B_PV, PosVel>(
+            b.nbr, n, i, cnt,
+            [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
+            [&](const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(P, pos, q.p)); });
         drho = P.mass * drho;
         drho += dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho = __ldg(&b.density[i]);
@@ -324,18 +391,16 @@ __device__ __forceinline__ F3 kappa_sum(const DevParams &P, const SimBufs &b, ui
                                         uint32_t n, F3 pos, float kd_i) {
     const uint32_t cnt = __ldg(&b.nbr_n[i]);
     F3 dv = f3(0.f, 0.f, 0.f);
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
-        const F3 e = pair_grad(P, pos, __ldg(&b.wpos[j]));
-        dv = dv + (kd_i + __ldg(&b.kd[j])) * e;
-    }
+    walk<FCU_B_KD, PosKd>(
+        b.nbr, n, i, cnt, [&](uint32_t j) { return PosKd{__ldg(&b.wpos[j]), __ldg(&b.kd[j])}; },
+        [&](const PosKd &q) { dv = dv + (kd_i + q.kd) * pair_grad(P, pos, q.p); });
     return dv;
 }
 
 // ---- apply_kappa_wide: div_apply / den_apply (sim_solve.wgsl:608-621) -----
 // For the density iterations the applied pressure k*rho that den_kappa held
 // back joins the pressure here, with the kappa it belongs to.
-__global__ void __launch_bounds__(kSolveThreads) k_apply(DevParams P, SimBufs b,
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_apply(DevParams P, SimBufs b,
                                                          const DevStep *__restrict__ st,
                                                          int add_pressure) {
     const uint32_t n = P.count;
@@ -353,7 +418,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_apply(DevParams P, SimBufs b,
 }
 
 // ---- forces_eval (sim_solve.wgsl:524-592) ---------------------------------
-__global__ void __launch_bounds__(kSolveThreads) k_forces_eval(DevParams P, SimBufs b) {
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_eval(DevParams P, SimBufs b) {
     const uint32_t n = P.count;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -378,26 +443,29 @@ __global__ void __launch_bounds__(kSolveThreads) k_forces_eval(DevParams P, SimB
     F3 visc = f3(0.f, 0.f, 0.f), blend = f3(0.f, 0.f, 0.f), near = f3(0.f, 0.f, 0.f),
        tension = f3(0.f, 0.f, 0.f);
     float heat = 0.0f;
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
-        const float4 pj = __ldg(&b.wpos[j]);
+    auto load = [&](uint32_t j) {
+        return Nbr5{__ldg(&b.wpos[j]), __ldg(&b.wvel[j]), __ldg(&b.density[j]), __ldg(&b.wtemp[j]),
+                    __ldg(&b.rho_near[j])};
+    };
+    walk<FCU_B_N5, Nbr5>(b.nbr, n, i, cnt, load, [&](const Nbr5 &q) {
+        const float4 pj = q.p;
         const F3 e = pair_grad(P, pos, pj);
         const F3 x = pos - xyz(pj);
         const float r2 = dot(x, x);
         const float r = sqrtf(r2);
-        const float rho_j = __ldg(&b.density[j]);
+        const float rho_j = q.rho;
         const float f = dot(x, e) / (r2 + 0.01f * P.h * P.h);
         const float pair = P.mass / (rho_i * rho_j) * f;
-        const F3 dv = vel - xyz(__ldg(&b.wvel[j]));
+        const F3 dv = vel - xyz(q.v);
         const float wn = fmaxf(1.0f - r * P.inv_h, 0.0f);
-        near = near + ((near_i + __ldg(&b.rho_near[j])) * wn * wn) * (x / fmaxf(r, 1e-5f));
+        near = near + ((near_i + q.near) * wn * wn) * (x / fmaxf(r, 1e-5f));
         visc = visc + (visc_k * pair) * dv;
         blend = blend - (P.mass / rho_j * kernel_q(P, r * P.inv_h)) * dv;
-        heat += heat_k * pair * (temp - __ldg(&b.wtemp[j]));
+        heat += heat_k * pair * (temp - q.temp);
         heat -= diss_k * pair * dot(dv, dv);
         const float corr = 2.0f * P.rho0 / (rho_i + rho_j);
         tension = tension - ((corr * P.mass * cohesion(r, coh_c, coh_k, coh_near)) * x) / fmaxf(r, 1e-9f);
-    }
+    });
     const F3 adh = (beta * P.rho0) * wall_adh_sum(P, pos);
     const F3 acc = visc + K_NEAR * near + gamma * tension + adh;
     b.accel[i] = make_float4(acc.x, acc.y, acc.z, heat);
@@ -428,7 +496,7 @@ __device__ __forceinline__ F3 fingers(const FluidStep &st, F3 pos, F3 v) {
 }
 
 // ---- forces_den_apply (sim_solve.wgsl:630-663) -----------------------------
-__global__ void __launch_bounds__(kSolveThreads) k_forces_apply(DevParams P, SimBufs b,
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_apply(DevParams P, SimBufs b,
                                                                 const DevStep *__restrict__ stp) {
     const uint32_t n = P.count;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -454,7 +522,7 @@ __global__ void __launch_bounds__(kSolveThreads) k_forces_apply(DevParams P, Sim
 }
 
 // ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
-__global__ void __launch_bounds__(kSolveThreads) k_den_kappa(DevParams P, SimBufs b,
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(DevParams P, SimBufs b,
                                                              const DevStep *__restrict__ st,
                                                              unsigned long long *acc) {
     const uint32_t n = P.count;
@@ -466,11 +534,10 @@ __global__ void __launch_bounds__(kSolveThreads) k_den_kappa(DevParams P, SimBuf
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
         float drho = 0.0f;
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const uint32_t j = __ldg(&b.nbr[(size_t)k * n + i]);
-            const F3 e = pair_grad(P, pos, __ldg(&b.wpos[j]));
-            drho += dot(vel - xyz(__ldg(&b.wvel[j])), e);
-        }
+        walk<FCU_B_PV, PosVel>(
+            b.nbr, n, i, cnt,
+            [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
+            [&](const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(P, pos, q.p)); });
         const float rho = __ldg(&b.density[i]);
         drho = P.mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;
