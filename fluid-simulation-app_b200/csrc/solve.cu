@@ -20,13 +20,13 @@
 // + velocity records, and forces_eval's five records; FCU_MINB is the
 // minimum resident blocks per SM the sweeps are compiled for (0: none).
 #ifndef FCU_B_KD
-#define FCU_B_KD 8
+#define FCU_B_KD 4
 #endif
 #ifndef FCU_B_PV
-#define FCU_B_PV 8
+#define FCU_B_PV 4
 #endif
 #ifndef FCU_B_N5
-#define FCU_B_N5 4
+#define FCU_B_N5 2
 #endif
 #ifndef FCU_MINB
 #define FCU_MINB 0
@@ -54,8 +54,11 @@ __device__ __forceinline__ float kernel_q(const DevParams &P, float q) {  // :17
     return P.sigma * 0.25f * t * t * t;
 }
 
-__device__ __forceinline__ F3 grad_q(const DevParams &P, F3 x, float r, float q) {  // :184-196
-    if (r < 1e-9f) return f3(0.f, 0.f, 0.f);
+// grad_q (sim_solve.wgsl:184-196) returns (dw / r) * x; this is its scalar
+// dw / r, and 0 under the r < 1e-9 guard (0 * x sums exactly like the
+// guard's zero vector: a signed zero added to any sum leaves it unchanged).
+__device__ __forceinline__ float grad_scale(const DevParams &P, float r, float q) {
+    if (r < 1e-9f) return 0.0f;
     float dw;
     if (q < 1.0f) {
         dw = P.sigma_h * (-3.0f * q + 2.25f * q * q);
@@ -63,7 +66,7 @@ __device__ __forceinline__ F3 grad_q(const DevParams &P, F3 x, float r, float q)
         const float t = 2.0f - q;
         dw = P.sigma_h * (-0.75f * t * t);
     }
-    return (dw / r) * x;
+    return dw / r;
 }
 
 __device__ __forceinline__ float cohesion(float r, float c, float k, float near) {  // :201-210
@@ -200,36 +203,33 @@ __device__ __forceinline__ float det_exp(float x) {
     return p * __uint_as_float((uint32_t)(k + 127) << 23);
 }
 
-// The neighbour's kernel gradient from the two positions (grad_q of
-// density_div's pair, recomputed).
-__device__ __forceinline__ F3 pair_grad(const DevParams &P, F3 pos, float4 pj) {
-    const F3 x = pos - xyz(pj);
-    const float r2 = dot(x, x);
-    const float r = sqrtf(r2);
-    const float q = r * P.inv_h;
-    return grad_q(P, x, r, q);
+// The neighbour's kernel gradient, bit for bit what grad_q returned for the
+// pair in density_div: its stored scale dw / r times x_i - x_j.
+__device__ __forceinline__ F3 pair_grad(float scale, F3 pos, float4 pj) {
+    return scale * (pos - xyz(pj));
 }
 
 // Walks particle i's neighbour list in list order, B entries at a time: the
-// B list words are loaded, then the B neighbours' records, and only then is
-// any of them used, so one batch's loads overlap instead of each neighbour
-// waiting on the round trip of the one before. The partial last batch loads
-// the particle's own record in its empty places and skips them. `use` sees
-// the neighbours in the same order as a plain loop, so every sum is the
-// same sum.
+// B list entries are loaded, then the B neighbours' records, and only then
+// is any of them used, so one batch's loads overlap instead of each
+// neighbour waiting on the round trip of the one before. The partial last
+// batch loads the particle's own record in its empty places and skips them.
+// `use(scale, record)` sees the neighbours in the same order as a plain
+// loop, so every sum is the same sum.
 template <int B, class T, class Load, class Use>
-__device__ __forceinline__ void walk(const uint32_t *__restrict__ nbr, uint32_t n, uint32_t i,
+__device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, uint32_t i,
                                      uint32_t cnt, Load load, Use use) {
     for (uint32_t k = 0; k < cnt; k += B) {
-        uint32_t j[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u) j[u] = (k + u < cnt) ? __ldg(&nbr[(size_t)(k + u) * n + i]) : i;
-        T v[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u) v[u] = load(j[u]);
+        uint2 e[B];
 #pragma unroll
         for (int u = 0; u < B; ++u)
-            if (k + u < cnt) use(v[u]);
+            e[u] = (k + u < cnt) ? __ldg(&nbr[(size_t)(k + u) * n + i]) : make_uint2(i, 0u);
+        T v[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) v[u] = load(e[u].x);
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (k + u < cnt) use(__uint_as_float(e[u].y), v[u]);
     }
 }
 
@@ -259,78 +259,175 @@ __global__ void __launch_bounds__(256) k_gather(SimBufs b, uint32_t n) {
     b.wid[k] = __ldg(&b.id[i]);
 }
 
+// One row (oz, oy) of a particle's 27-cell stencil: three x-adjacent cells,
+// one contiguous slot range of the cell-ordered working set. Cell culling: a
+// stencil cell whose nearest point lies beyond the support holds no
+// neighbour, so skipping it changes neither the neighbour set nor its order.
+// The distances to the own cell's faces are shrunk by a margin far above
+// their rounding error (1e-3 cell plus 1e-6 |pos|, ~8 ulp of the
+// coordinates), so a cell is culled only when every candidate in it would
+// fail r2 < support^2. Returns false for a row outside the grid or culled.
+struct Stencil {
+    int bx, by, bz;
+    float xl, xh, yl, yh, zl, zh;
+};
+
+__device__ __forceinline__ Stencil stencil_of(const DevParams &P, F3 pos) {
+    Stencil t;
+    t.bx = (int)axis_cell(pos.x, P.box_min[0], P.cell, P.dims[0]);
+    t.by = (int)axis_cell(pos.y, P.box_min[1], P.cell, P.dims[1]);
+    t.bz = (int)axis_cell(pos.z, P.box_min[2], P.cell, P.dims[2]);
+    const float margin = 1e-3f * P.cell + 1e-6f * (fabsf(pos.x) + fabsf(pos.y) + fabsf(pos.z));
+    const float fx = pos.x - (P.box_min[0] + (float)t.bx * P.cell);
+    const float fy = pos.y - (P.box_min[1] + (float)t.by * P.cell);
+    const float fz = pos.z - (P.box_min[2] + (float)t.bz * P.cell);
+    t.xl = fmaxf(fx - margin, 0.0f);
+    t.xh = fmaxf(P.cell - fx - margin, 0.0f);
+    t.yl = fmaxf(fy - margin, 0.0f);
+    t.yh = fmaxf(P.cell - fy - margin, 0.0f);
+    t.zl = fmaxf(fz - margin, 0.0f);
+    t.zh = fmaxf(P.cell - fz - margin, 0.0f);
+    return t;
+}
+
+__device__ __forceinline__ bool stencil_row(const DevParams &P, const uint32_t *__restrict__ starts,
+                                            uint32_t n, const Stencil &t, int oz, int oy,
+                                            uint32_t &s, uint32_t &e, uint32_t &rowkey) {
+    const int cz = t.bz + oz, cy = t.by + oy;
+    if (cz < 0 || cz >= (int)P.dims[2] || cy < 0 || cy >= (int)P.dims[1]) return false;
+    const float dzp = oz < 0 ? t.zl * t.zl : (oz > 0 ? t.zh * t.zh : 0.0f);
+    const float dperp = dzp + (oy < 0 ? t.yl * t.yl : (oy > 0 ? t.yh * t.yh : 0.0f));
+    if (dperp >= P.support_sq) return false;
+    const int cx0 = (t.bx > 0 && dperp + t.xl * t.xl < P.support_sq) ? t.bx - 1 : t.bx;
+    const int cx1 = (t.bx + 1 < (int)P.dims[0] && dperp + t.xh * t.xh < P.support_sq) ? t.bx + 1 : t.bx;
+    rowkey = ((uint32_t)cz * P.dims[1] + (uint32_t)cy) * P.dims[0];
+    s = __ldg(&starts[rowkey + cx0]);
+    e = __ldg(&starts[rowkey + cx1 + 1]);
+    if (e > n) e = n;  // starts never exceed n unless a scan gave up
+    return s < e;
+}
+
+// The pair terms density_div sums over one neighbour (sim_solve.wgsl:449-466).
+struct DensitySums {
+    float w_sum, rho_near, grad_sq, drho;
+    F3 grad_sum;
+};
+
+__device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d, F3 pos, F3 vel,
+                                              F3 x, float r2, float4 vj) {
+    const float r = sqrtf(r2);
+    const float q = r * P.inv_h;
+    d.w_sum += kernel_q(P, q);
+    const float wn = fmaxf(1.0f - q, 0.0f);
+    d.rho_near += wn * wn * wn;
+    const float gs = grad_scale(P, r, q);
+    const F3 gw = gs * x;
+    d.grad_sum = d.grad_sum + gw;
+    d.grad_sq += dot(gw, gw);
+    d.drho += dot(vel - xyz(vj), gw);
+    return gs;
+}
+
 // ---- density_div (sim_solve.wgsl:411-518) --------------------------------
+// Two phases. (1) The candidate scan, warp-uniform: lanes whose stencil row
+// is the same cell row walk the union of their slot ranges together, one
+// broadcast load per candidate, each lane keeping its own candidates; hits
+// are appended to the lane's list in row order, slots ascending, the order a
+// per-particle loop finds them. (2) Each lane walks its own hits and forms
+// the sums. A particle with more neighbours than the list holds rescans its
+// stencil in phase 2, so its sums still see every neighbour.
 __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimBufs b,
                                                                const DevStep *__restrict__ st,
                                                                DevSolve *solve,
                                                                unsigned long long *acc) {
     const uint32_t n = P.count;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const uint32_t lane = threadIdx.x & 31;
     const float dt = st->s.dt;
-    unsigned long long term = 0;
-    if (i < n) {
-        const float4 *__restrict__ wpos = b.wpos;
-        const float4 *__restrict__ wvel = b.wvel;
-        const F3 pos = xyz(__ldg(&wpos[i]));
-        const F3 vel = xyz(__ldg(&wvel[i]));
-        const int bx = (int)axis_cell(pos.x, P.box_min[0], P.cell, P.dims[0]);
-        const int by = (int)axis_cell(pos.y, P.box_min[1], P.cell, P.dims[1]);
-        const int bz = (int)axis_cell(pos.z, P.box_min[2], P.cell, P.dims[2]);
-        const int dx = (int)P.dims[0], dy = (int)P.dims[1], dz = (int)P.dims[2];
-        // Cell culling: a stencil cell whose nearest point lies beyond the
-        // support holds no neighbour, so skipping it changes neither the
-        // neighbour set nor its order. The distances to the own cell's faces
-        // are shrunk by a margin far above their rounding error (1e-3 cell
-        // plus 1e-6 |pos|, ~8 ulp of the coordinates), so a cell is culled
-        // only when every candidate in it would fail r2 < support^2.
-        const float margin = 1e-3f * P.cell + 1e-6f * (fabsf(pos.x) + fabsf(pos.y) + fabsf(pos.z));
-        const float fx = pos.x - (P.box_min[0] + (float)bx * P.cell);
-        const float fy = pos.y - (P.box_min[1] + (float)by * P.cell);
-        const float fz = pos.z - (P.box_min[2] + (float)bz * P.cell);
-        const float xl = fmaxf(fx - margin, 0.0f), xh = fmaxf(P.cell - fx - margin, 0.0f);
-        const float yl = fmaxf(fy - margin, 0.0f), yh = fmaxf(P.cell - fy - margin, 0.0f);
-        const float zl = fmaxf(fz - margin, 0.0f), zh = fmaxf(P.cell - fz - margin, 0.0f);
-        float w_sum = P.sigma;
-        float rho_near = 0.0f;
-        F3 grad_sum = f3(0.f, 0.f, 0.f);
-        float grad_sq = 0.0f;
-        float drho = 0.0f;
-        uint32_t found = 0;
-        const uint32_t cap = P.nbr_cap;
-        for (int oz = -1; oz <= 1; ++oz) {
-            const int cz = bz + oz;
-            if (cz < 0 || cz >= dz) continue;
-            const float dzp = oz < 0 ? zl * zl : (oz > 0 ? zh * zh : 0.0f);
-            for (int oy = -1; oy <= 1; ++oy) {
-                const int cy = by + oy;
-                if (cy < 0 || cy >= dy) continue;
-                const float dperp = dzp + (oy < 0 ? yl * yl : (oy > 0 ? yh * yh : 0.0f));
-                if (dperp >= P.support_sq) continue;
-                const int cx0 = (bx > 0 && dperp + xl * xl < P.support_sq) ? bx - 1 : bx;
-                const int cx1 = (bx + 1 < dx && dperp + xh * xh < P.support_sq) ? bx + 1 : bx;
-                const uint32_t row = ((uint32_t)cz * (uint32_t)dy + (uint32_t)cy) * (uint32_t)dx;
-                const uint32_t s = __ldg(&b.starts[row + cx0]);
-                uint32_t e = __ldg(&b.starts[row + cx1 + 1]);
-                if (e > n) e = n;  // starts never exceed n unless a scan gave up
-                for (uint32_t k = s; k < e; ++k) {
-                    if (k == i) continue;
-                    const F3 x = pos - xyz(__ldg(&wpos[k]));
-                    const float r2 = dot(x, x);
-                    if (r2 >= P.support_sq) continue;
-                    const float r = sqrtf(r2);
-                    const float q = r * P.inv_h;
-                    w_sum += kernel_q(P, q);
-                    const float wn = fmaxf(1.0f - q, 0.0f);
-                    rho_near += wn * wn * wn;
-                    const F3 gw = grad_q(P, x, r, q);
-                    grad_sum = grad_sum + gw;
-                    grad_sq += dot(gw, gw);
-                    drho += dot(vel - xyz(__ldg(&wvel[k])), gw);
-                    if (found < cap) b.nbr[(size_t)found * n + i] = k;
-                    found++;
+    const float4 *__restrict__ wpos = b.wpos;
+    const float4 *__restrict__ wvel = b.wvel;
+    const uint32_t me = live ? i : 0u;  // lanes past n scan nothing
+    const F3 pos = xyz(__ldg(&wpos[me]));
+    const Stencil t = stencil_of(P, pos);
+    const uint32_t cap = P.nbr_cap;
+    uint32_t found = 0;
+    for (int oz = -1; oz <= 1; ++oz) {
+        for (int oy = -1; oy <= 1; ++oy) {
+            uint32_t s = 0, e = 0, rowkey = 0;
+            const bool ok = live && stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey);
+            uint32_t pending = __ballot_sync(0xffffffffu, ok);
+            while (pending) {
+                const int leader = __ffs(pending) - 1;
+                const uint32_t lkey = __shfl_sync(0xffffffffu, rowkey, leader);
+                const bool mine = ok && ((pending >> lane) & 1u) && rowkey == lkey;
+                const uint32_t group = __ballot_sync(0xffffffffu, mine);
+                const uint32_t S = __reduce_min_sync(0xffffffffu, mine ? s : 0xffffffffu);
+                const uint32_t E = __reduce_max_sync(0xffffffffu, mine ? e : 0u);
+                for (uint32_t k = S; k < E; ++k) {
+                    const float4 p = __ldg(&wpos[k]);
+                    if (mine && k >= s && k < e && k != i) {
+                        const F3 x = pos - xyz(p);
+                        if (dot(x, x) < P.support_sq) {
+                            if (found < cap) b.nbr[(size_t)found * n + i].x = k;
+                            found++;
+                        }
+                    }
                 }
+                pending &= ~group;
             }
         }
+    }
+    unsigned long long term = 0;
+    if (live) {
+        const F3 vel = xyz(__ldg(&wvel[i]));
+        DensitySums d;
+        d.w_sum = P.sigma;
+        d.rho_near = 0.0f;
+        d.grad_sq = 0.0f;
+        d.drho = 0.0f;
+        d.grad_sum = f3(0.f, 0.f, 0.f);
+        if (found <= cap) {
+            constexpr int B = 4;
+            for (uint32_t k = 0; k < found; k += B) {
+                uint32_t j[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) j[u] = (k + u < found) ? b.nbr[(size_t)(k + u) * n + i].x : i;
+                float4 pj[B], vj[B];
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    pj[u] = __ldg(&wpos[j[u]]);
+                    vj[u] = __ldg(&wvel[j[u]]);
+                }
+#pragma unroll
+                for (int u = 0; u < B; ++u) {
+                    if (k + u < found) {
+                        const F3 x = pos - xyz(pj[u]);
+                        const float gs = density_pair(P, d, pos, vel, x, dot(x, x), vj[u]);
+                        b.nbr[(size_t)(k + u) * n + i] = make_uint2(j[u], __float_as_uint(gs));
+                    }
+                }
+            }
+        } else {
+            // more neighbours than the list holds: rescan, summing all
+            uint32_t seen = 0;
+            for (int oz = -1; oz <= 1; ++oz)
+                for (int oy = -1; oy <= 1; ++oy) {
+                    uint32_t s, e, rowkey;
+                    if (!stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey)) continue;
+                    for (uint32_t k = s; k < e; ++k) {
+                        if (k == i) continue;
+                        const F3 x = pos - xyz(__ldg(&wpos[k]));
+                        const float r2 = dot(x, x);
+                        if (r2 >= P.support_sq) continue;
+                        const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&wvel[k]));
+                        if (seen < cap) b.nbr[(size_t)seen * n + i] = make_uint2(k, __float_as_uint(gs));
+                        seen++;
+                    }
+                }
+        }
+        float w_sum = d.w_sum, rho_near = d.rho_near, grad_sq = d.grad_sq, drho = d.drho;
+        F3 grad_sum = d.grad_sum;
         b.nbr_n[i] = found < cap ? found : cap;
         if (found > cap) atomicAdd(&solve->nbr_over, found - cap);
         float rho = P.mass * w_sum;
@@ -376,7 +473,7 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(DevParams
         walk<FCU_B_PV, PosVel>(
             b.nbr, n, i, cnt,
             [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
-            [&](const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(P, pos, q.p)); });
+            [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
         drho = P.mass * drho;
         drho += dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho = __ldg(&b.density[i]);
@@ -393,7 +490,7 @@ __device__ __forceinline__ F3 kappa_sum(const DevParams &P, const SimBufs &b, ui
     F3 dv = f3(0.f, 0.f, 0.f);
     walk<FCU_B_KD, PosKd>(
         b.nbr, n, i, cnt, [&](uint32_t j) { return PosKd{__ldg(&b.wpos[j]), __ldg(&b.kd[j])}; },
-        [&](const PosKd &q) { dv = dv + (kd_i + q.kd) * pair_grad(P, pos, q.p); });
+        [&](float gs, const PosKd &q) { dv = dv + (kd_i + q.kd) * pair_grad(gs, pos, q.p); });
     return dv;
 }
 
@@ -447,9 +544,9 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_eval(DevPara
         return Nbr5{__ldg(&b.wpos[j]), __ldg(&b.wvel[j]), __ldg(&b.density[j]), __ldg(&b.wtemp[j]),
                     __ldg(&b.rho_near[j])};
     };
-    walk<FCU_B_N5, Nbr5>(b.nbr, n, i, cnt, load, [&](const Nbr5 &q) {
+    walk<FCU_B_N5, Nbr5>(b.nbr, n, i, cnt, load, [&](float gs, const Nbr5 &q) {
         const float4 pj = q.p;
-        const F3 e = pair_grad(P, pos, pj);
+        const F3 e = pair_grad(gs, pos, pj);
         const F3 x = pos - xyz(pj);
         const float r2 = dot(x, x);
         const float r = sqrtf(r2);
@@ -537,7 +634,7 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(DevParams
         walk<FCU_B_PV, PosVel>(
             b.nbr, n, i, cnt,
             [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
-            [&](const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(P, pos, q.p)); });
+            [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
         const float rho = __ldg(&b.density[i]);
         drho = P.mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;

@@ -19,7 +19,12 @@ struct SimBufs {
     uint32_t *keys, *starts, *perm;
     float *density, *alpha, *kd, *pressure, *pinc, *rho_near;
     float4 *accel, *xsph, *wgrad;
-    uint32_t *nbr, *nbr_n;
+    // Neighbour list, slot-major (entry k of particle i at k * n + i): the
+    // neighbour's slot and the bits of its kernel-gradient scale dw / r,
+    // so a sweep forms the gradient (dw / r) * (x_i - x_j) without the
+    // square root and the division density_div already did.
+    uint2 *nbr;
+    uint32_t *nbr_n;
     // tracers
     uint32_t *tracers;  // 2 words each
     int32_t *vel_grid;  // 4 per cell, atomic sums

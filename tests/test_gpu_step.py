@@ -241,3 +241,19 @@ def test_the_tolerance_schedule_matches_the_oracle(fcu, orc, tols):
         seen.add(int(iters[1]))
     same_state(sim, o, "tolerance")
     assert len(seen) > 1, "the iteration count never varied"
+
+
+# A list cap below the neighbour count (sim_solve.wgsl:384-388): every
+# particle keeps its first cap neighbours for the later sweeps, the density
+# sums still see all of them, and the overflow is counted.
+def test_neighbour_overflow_matches_the_oracle(fcu, orc):
+    sim, o = pair(fcu, orc, nbr_cap=20)
+    dt = frame_dt(7)
+    s_g, s_o = step_pair(fcu, orc, force=(0, -9.81, 0), dt=dt, v_clamp=v_clamp(TB["spacing"], dt))
+    sim.run([s_g] * 5)
+    for _ in range(5):
+        o.substep(s_o)
+    for f in ("density", "alpha", "nbr_n", "counters"):
+        assert_same_bits(sim.field(f), o.field(f), f)
+    assert sim.field("counters")[1] > 0
+    same_state(sim, o, "overflow")
