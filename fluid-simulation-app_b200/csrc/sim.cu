@@ -456,34 +456,43 @@ int32_t upload_steps(FluidSim *s, const FluidStep *steps, uint32_t count) {
     return FLUID_OK;
 }
 
-// The substep policy of render.rs:57-106, in f32 as the reference computes it.
-constexpr float kSubstepPerSpacing = 0.42f;  // render.rs:56
-constexpr float kRefineShortDt = 0.00105f;   // render.rs:69
-constexpr float kNominalFrame = 1.0f / 120.0f;
-constexpr float kCheapRungCost = 0.65f;      // render.rs:86
-
-uint32_t sat_u32f(float v) {  // Rust's saturating `as u32`
-    if (!(v > 0.0f)) return 0u;
-    if (v >= 4294967296.0f) return 0xffffffffu;
-    return (uint32_t)v;
-}
-
-uint32_t substep_floor(float dt, float dt_sub_max) {  // render.rs:63-65
-    const uint32_t n = sat_u32f(std::ceil(dt / dt_sub_max));
-    return n < 8u ? n : 8u;
-}
-
-uint32_t refine_passes(float dt_sub) { return dt_sub > kRefineShortDt ? 5u : 2u; }  // :76-78
-
-uint32_t substeps_for(float dt, float v_max, float spacing, uint32_t cap) {  // :97-106
-    uint32_t n = sat_u32f(std::ceil(dt * v_max / (0.4f * spacing)));
-    const uint32_t fl = substep_floor(dt, kSubstepPerSpacing * spacing);
-    if (fl > n) n = fl;
-    const uint32_t cheap = sat_u32f(std::ceil(kNominalFrame / kRefineShortDt));
-    const bool jump = refine_passes(dt / (float)cheap) == 2u && n < cheap &&
-                      (float)n > kCheapRungCost * (float)cheap;
-    if (jump) n = cheap;
-    return n < cap ? n : cap;
+// One frame on the GPU (render.rs:3168-3229 minus drawing): n substeps of
+// the Step block `st` (the fixed schedule runs `refine` density pairs), then
+// reduce_stats, a tracer pass at the frame dt and seed, and the stale-stats
+// copy the next frame's substep policy reads without blocking.
+int32_t run_frame(FluidSim *s, const FluidStep &st, uint32_t n, uint32_t refine, float frame_dt,
+                  uint32_t seed) {
+    std::vector<FluidStep> steps(n, st);
+    int32_t rc = upload_steps(s, steps.data(), n);
+    if (rc != FLUID_OK) return rc;
+    cudaGraphExec_t g;
+    rc = substep_graph(s, refine, &g);
+    if (rc != FLUID_OK) return rc;
+    for (uint32_t k = 0; k < n; ++k) CK(cudaGraphLaunch(g, s->stream));
+    launch_stats(s->stream, s->P, s->b, s->solve);
+    if (s->ntr) {
+        FluidStep tr;
+        std::memset(&tr, 0, sizeof tr);
+        tr.force[0] = st.force[0];
+        tr.force[1] = st.force[1];
+        tr.force[2] = st.force[2];
+        tr.dt = frame_dt;
+        tr.seed = seed;
+        DevStep d;
+        fill_step(s, tr, d);
+        launch_splat(s->stream, s->P, s->b);
+        launch_resolve(s->stream, s->P, s->b);
+        launch_advect(s->stream, s->P, s->b, d, s->ntr);
+    }
+    CK(cudaGetLastError());
+    if (!s->stats_pending) {
+        CK(cudaMemcpyAsync(s->h_stats_stale, s->b.stats, 16 * sizeof(float), cudaMemcpyDeviceToHost,
+                           s->stream));
+        CK(cudaEventRecord(s->stats_ready, s->stream));
+        s->stats_pending = true;
+    }
+    s->last_frame_substeps = n;
+    return FLUID_OK;
 }
 
 bool valid_config(const FluidSimConfig *c, std::string &why) {
@@ -575,6 +584,7 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     if ((uint64_t)s->n * cfg->nbr_cap > (1ull << 40)) return fail(FLUID_ERR_ARG, "neighbour lists too large");
 
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CK(density_div_prepare(cfg->nbr_cap));
     const size_t n = s->n, C = s->cells;
     SimBufs &b = s->b;
     CK(s->alloc(&b.pos, n));
@@ -959,55 +969,40 @@ int32_t fluid_sim_frame(FluidSim *s, FluidVec3 force, FluidVec3 omega, FluidVec3
         return FLUID_OK;
     }
     uint32_t n = substeps ? substeps
-                          : substeps_for(dt, s->v_max_stale, s->cfg.spacing, cap ? cap : 16u);
+                          : fluid_substeps_for(dt, s->v_max_stale, s->cfg.spacing, cap ? cap : 16u);
     if (n == 0) n = 1;
     const float dt_sub = dt / (float)n;
-    const float v_clamp = 0.4f * s->cfg.spacing / dt_sub;  // render.rs:3171
-    std::vector<FluidStep> steps(n);
-    for (auto &st : steps) {
-        std::memset(&st, 0, sizeof st);
-        st.force[0] = force.x;
-        st.force[1] = force.y;
-        st.force[2] = force.z;
-        st.dt = dt_sub;
-        st.omega[0] = omega.x;
-        st.omega[1] = omega.y;
-        st.omega[2] = omega.z;
-        st.v_clamp = v_clamp;
-        st.domega[0] = domega.x;
-        st.domega[1] = domega.y;
-        st.domega[2] = domega.z;
+    FluidStep st;
+    std::memset(&st, 0, sizeof st);
+    st.force[0] = force.x;
+    st.force[1] = force.y;
+    st.force[2] = force.z;
+    st.dt = dt_sub;
+    st.omega[0] = omega.x;
+    st.omega[1] = omega.y;
+    st.omega[2] = omega.z;
+    st.v_clamp = 0.4f * s->cfg.spacing / dt_sub;  // render.rs:3171
+    st.domega[0] = domega.x;
+    st.domega[1] = domega.y;
+    st.domega[2] = domega.z;
+    return run_frame(s, st, n, fluid_refine_passes(dt_sub), dt, seed);
+}
+
+int32_t fluid_sim_frame_plan(FluidSim *s, const FluidFramePlan *plan) {
+    if (!s || !plan) return fail(FLUID_ERR_ARG, "null argument");
+    CK(cudaSetDevice(s->device));
+    if (s->stats_pending && cudaEventQuery(s->stats_ready) == cudaSuccess) {
+        s->v_max_stale = s->h_stats_stale[6];
+        s->stats_pending = false;
     }
-    int32_t rc = upload_steps(s, steps.data(), n);
-    if (rc != FLUID_OK) return rc;
-    cudaGraphExec_t g;
-    rc = substep_graph(s, refine_passes(dt_sub), &g);
-    if (rc != FLUID_OK) return rc;
-    for (uint32_t k = 0; k < n; ++k) CK(cudaGraphLaunch(g, s->stream));
-    launch_stats(s->stream, s->P, s->b, s->solve);
-    if (s->ntr) {
-        FluidStep tr;
-        std::memset(&tr, 0, sizeof tr);
-        tr.force[0] = force.x;
-        tr.force[1] = force.y;
-        tr.force[2] = force.z;
-        tr.dt = dt;
-        tr.seed = seed;
-        DevStep d;
-        fill_step(s, tr, d);
-        launch_splat(s->stream, s->P, s->b);
-        launch_resolve(s->stream, s->P, s->b);
-        launch_advect(s->stream, s->P, s->b, d, s->ntr);
+    if (plan->asleep || plan->dt == 0.0f || plan->substeps == 0) {
+        s->last_frame_substeps = 0;
+        return FLUID_OK;
     }
-    CK(cudaGetLastError());
-    if (!s->stats_pending) {
-        CK(cudaMemcpyAsync(s->h_stats_stale, s->b.stats, 16 * sizeof(float), cudaMemcpyDeviceToHost,
-                           s->stream));
-        CK(cudaEventRecord(s->stats_ready, s->stream));
-        s->stats_pending = true;
-    }
-    s->last_frame_substeps = n;
-    return FLUID_OK;
+    if (!std::isfinite(plan->dt) || plan->dt < 0.0f || !(plan->step.dt > 0.0f))
+        return fail(FLUID_ERR_ARG, "plan dt must be finite and positive");
+    return run_frame(s, plan->step, plan->substeps, plan->refine ? plan->refine : 5u, plan->dt,
+                     plan->seed);
 }
 
 uint64_t fluid_grid_workspace_bytes(uint32_t n, const FluidGrid *grid) {

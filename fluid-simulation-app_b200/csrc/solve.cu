@@ -329,33 +329,129 @@ __device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d
 }
 
 // ---- density_div (sim_solve.wgsl:411-518) --------------------------------
+
+// The single-pass scan: every candidate of the stencil, in order, each hit
+// summed and listed (the first `cap` of them). Returns the hits found.
+__device__ __forceinline__ uint32_t density_scan(const DevParams &P, const SimBufs &b, uint32_t i,
+                                                 F3 pos, F3 vel, const Stencil &t, DensitySums &d) {
+    const uint32_t n = P.count, cap = P.nbr_cap;
+    uint32_t seen = 0;
+    for (int oz = -1; oz <= 1; ++oz)
+        for (int oy = -1; oy <= 1; ++oy) {
+            uint32_t s, e, rowkey;
+            if (!stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey)) continue;
+            for (uint32_t k = s; k < e; ++k) {
+                if (k == i) continue;
+                const F3 x = pos - xyz(__ldg(&b.wpos[k]));
+                const float r2 = dot(x, x);
+                if (r2 >= P.support_sq) continue;
+                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
+                if (seen < cap) b.nbr[(size_t)seen * n + i] = make_uint2(k, __float_as_uint(gs));
+                seen++;
+            }
+        }
+    return seen;
+}
+
+__device__ __forceinline__ DensitySums density_sums_init(const DevParams &P) {
+    DensitySums d;
+    d.w_sum = P.sigma;  // lane 0's self term W(0), sim_solve.wgsl:426
+    d.rho_near = 0.0f;
+    d.grad_sq = 0.0f;
+    d.drho = 0.0f;
+    d.grad_sum = f3(0.f, 0.f, 0.f);
+    return d;
+}
+
+// Everything density_div does after its neighbour sums (sim_solve.wgsl:
+// 475-517): list length and overflow, density with the wall fill, the wall
+// gradient, alpha, the divergence kappa; returns the residual term.
+__device__ __forceinline__ unsigned long long density_finish(const DevParams &P, const SimBufs &b,
+                                                             uint32_t i, F3 pos, F3 vel,
+                                                             const DensitySums &d, uint32_t found,
+                                                             float dt, DevSolve *solve) {
+    const uint32_t cap = P.nbr_cap;
+    b.nbr_n[i] = found < cap ? found : cap;
+    if (found > cap) atomicAdd(&solve->nbr_over, found - cap);
+    float rho = P.mass * d.w_sum;
+    const float rho_near = d.rho_near;
+    const float grad_sq = P.mass * P.mass * d.grad_sq;
+    float drho = P.mass * d.drho;
+    F3 grad_sum = P.mass * d.grad_sum;
+    const F3 lo = wall_lo(P), hi = wall_hi(P);
+    const F3 tl = (pos - lo) * P.inv_h;
+    const F3 th = (hi - pos) * P.inv_h;
+    float fill = 0.0f;
+    fill += wall_density(tl.x) + wall_density(th.x);
+    fill += wall_density(tl.y) + wall_density(th.y);
+    fill += wall_density(tl.z) + wall_density(th.z);
+    fill -= wedge_sum(tl, th);
+    rho += P.rho0 * fill;
+    const F3 wg = wall_grad_sum(P, pos);
+    b.wgrad[i] = make_float4(wg.x, wg.y, wg.z, 0.0f);
+    grad_sum = grad_sum + wg;
+    b.density[i] = rho;
+    b.rho_near[i] = rho_near;
+    const float a = rho / fmaxf(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
+    b.alpha[i] = a;
+    drho += dot(vel, wg);
+    b.kd[i] = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
+    return fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
+}
+
+// One thread per particle, the scan above: the path for neighbour caps too
+// large for the staged kernel's shared memory.
+__global__ void __launch_bounds__(kSolveThreads) k_density_div_scan(DevParams P, SimBufs b,
+                                                                    const DevStep *__restrict__ st,
+                                                                    DevSolve *solve,
+                                                                    unsigned long long *acc) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long term = 0;
+    if (i < P.count) {
+        const F3 pos = xyz(__ldg(&b.wpos[i]));
+        const F3 vel = xyz(__ldg(&b.wvel[i]));
+        DensitySums d = density_sums_init(P);
+        const uint32_t found = density_scan(P, b, i, pos, vel, stencil_of(P, pos), d);
+        term = density_finish(P, b, i, pos, vel, d, found, st->s.dt, solve);
+    }
+    accumulate_fixed(acc, term);
+}
+
 // Two phases. (1) The candidate scan, warp-uniform: lanes whose stencil row
 // is the same cell row walk the union of their slot ranges together, one
-// broadcast load per candidate, each lane keeping its own candidates; hits
-// are appended to the lane's list in row order, slots ascending, the order a
-// per-particle loop finds them. (2) Each lane walks its own hits and forms
-// the sums. A particle with more neighbours than the list holds rescans its
-// stencil in phase 2, so its sums still see every neighbour.
-__global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimBufs b,
-                                                               const DevStep *__restrict__ st,
-                                                               DevSolve *solve,
-                                                               unsigned long long *acc) {
+// broadcast load per candidate, each lane keeping its own candidates. A
+// lane's hits go to its own column of shared memory as (row, offset) codes,
+// in row order, slots ascending: the order a per-particle loop finds them.
+// (2) Each lane walks its hits and forms the sums; the lanes advance through
+// their lists together, so the list stores coalesce. A particle with more
+// neighbours than the list holds, or a stencil row longer than 4,096 slots,
+// rescans in phase 2, so its sums still see every neighbour.
+constexpr uint32_t kRowSpan = 4096;  // (row, offset) code: 4 + 12 bits
+
+__global__ void __launch_bounds__(kSolveThreads, 6) k_density_div(DevParams P, SimBufs b,
+                                                                  const DevStep *__restrict__ st,
+                                                                  DevSolve *solve,
+                                                                  unsigned long long *acc) {
+    extern __shared__ uint32_t dyn[];
+    uint32_t *s_row = dyn;                                         // [9][threads]
+    uint16_t *s_hit = reinterpret_cast<uint16_t *>(dyn + 9 * kSolveThreads);  // [cap][threads]
     const uint32_t n = P.count;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + tid;
     const bool live = i < n;
-    const uint32_t lane = threadIdx.x & 31;
-    const float dt = st->s.dt;
-    const float4 *__restrict__ wpos = b.wpos;
-    const float4 *__restrict__ wvel = b.wvel;
-    const uint32_t me = live ? i : 0u;  // lanes past n scan nothing
-    const F3 pos = xyz(__ldg(&wpos[me]));
+    const uint32_t lane = tid & 31;
+    const F3 pos = xyz(__ldg(&b.wpos[live ? i : 0u]));  // lanes past n scan nothing
     const Stencil t = stencil_of(P, pos);
     const uint32_t cap = P.nbr_cap;
     uint32_t found = 0;
+    bool wide = false;
+    int r = 0;
     for (int oz = -1; oz <= 1; ++oz) {
-        for (int oy = -1; oy <= 1; ++oy) {
+        for (int oy = -1; oy <= 1; ++oy, ++r) {
             uint32_t s = 0, e = 0, rowkey = 0;
             const bool ok = live && stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey);
+            s_row[r * kSolveThreads + tid] = s;
+            if (ok && e - s > kRowSpan) wide = true;
             uint32_t pending = __ballot_sync(0xffffffffu, ok);
             while (pending) {
                 const int leader = __ffs(pending) - 1;
@@ -365,11 +461,12 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimB
                 const uint32_t S = __reduce_min_sync(0xffffffffu, mine ? s : 0xffffffffu);
                 const uint32_t E = __reduce_max_sync(0xffffffffu, mine ? e : 0u);
                 for (uint32_t k = S; k < E; ++k) {
-                    const float4 p = __ldg(&wpos[k]);
+                    const float4 p = __ldg(&b.wpos[k]);
                     if (mine && k >= s && k < e && k != i) {
                         const F3 x = pos - xyz(p);
                         if (dot(x, x) < P.support_sq) {
-                            if (found < cap) b.nbr[(size_t)found * n + i].x = k;
+                            if (found < cap && !wide)
+                                s_hit[found * kSolveThreads + tid] = (uint16_t)((r << 12) | (k - s));
                             found++;
                         }
                     }
@@ -380,24 +477,22 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimB
     }
     unsigned long long term = 0;
     if (live) {
-        const F3 vel = xyz(__ldg(&wvel[i]));
-        DensitySums d;
-        d.w_sum = P.sigma;
-        d.rho_near = 0.0f;
-        d.grad_sq = 0.0f;
-        d.drho = 0.0f;
-        d.grad_sum = f3(0.f, 0.f, 0.f);
-        if (found <= cap) {
-            constexpr int B = 4;
+        const F3 vel = xyz(__ldg(&b.wvel[i]));
+        DensitySums d = density_sums_init(P);
+        if (found <= cap && !wide) {
+            constexpr int B = 2;
             for (uint32_t k = 0; k < found; k += B) {
                 uint32_t j[B];
 #pragma unroll
-                for (int u = 0; u < B; ++u) j[u] = (k + u < found) ? b.nbr[(size_t)(k + u) * n + i].x : i;
+                for (int u = 0; u < B; ++u) {
+                    const uint32_t code = k + u < found ? s_hit[(k + u) * kSolveThreads + tid] : 0u;
+                    j[u] = k + u < found ? s_row[(code >> 12) * kSolveThreads + tid] + (code & 4095u) : i;
+                }
                 float4 pj[B], vj[B];
 #pragma unroll
                 for (int u = 0; u < B; ++u) {
-                    pj[u] = __ldg(&wpos[j[u]]);
-                    vj[u] = __ldg(&wvel[j[u]]);
+                    pj[u] = __ldg(&b.wpos[j[u]]);
+                    vj[u] = __ldg(&b.wvel[j[u]]);
                 }
 #pragma unroll
                 for (int u = 0; u < B; ++u) {
@@ -409,50 +504,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimB
                 }
             }
         } else {
-            // more neighbours than the list holds: rescan, summing all
-            uint32_t seen = 0;
-            for (int oz = -1; oz <= 1; ++oz)
-                for (int oy = -1; oy <= 1; ++oy) {
-                    uint32_t s, e, rowkey;
-                    if (!stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey)) continue;
-                    for (uint32_t k = s; k < e; ++k) {
-                        if (k == i) continue;
-                        const F3 x = pos - xyz(__ldg(&wpos[k]));
-                        const float r2 = dot(x, x);
-                        if (r2 >= P.support_sq) continue;
-                        const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&wvel[k]));
-                        if (seen < cap) b.nbr[(size_t)seen * n + i] = make_uint2(k, __float_as_uint(gs));
-                        seen++;
-                    }
-                }
+            found = density_scan(P, b, i, pos, vel, t, d);
         }
-        float w_sum = d.w_sum, rho_near = d.rho_near, grad_sq = d.grad_sq, drho = d.drho;
-        F3 grad_sum = d.grad_sum;
-        b.nbr_n[i] = found < cap ? found : cap;
-        if (found > cap) atomicAdd(&solve->nbr_over, found - cap);
-        float rho = P.mass * w_sum;
-        grad_sq = P.mass * P.mass * grad_sq;
-        drho = P.mass * drho;
-        grad_sum = P.mass * grad_sum;
-        const F3 lo = wall_lo(P), hi = wall_hi(P);
-        const F3 tl = (pos - lo) * P.inv_h;
-        const F3 th = (hi - pos) * P.inv_h;
-        float fill = 0.0f;
-        fill += wall_density(tl.x) + wall_density(th.x);
-        fill += wall_density(tl.y) + wall_density(th.y);
-        fill += wall_density(tl.z) + wall_density(th.z);
-        fill -= wedge_sum(tl, th);
-        rho += P.rho0 * fill;
-        const F3 wg = wall_grad_sum(P, pos);
-        b.wgrad[i] = make_float4(wg.x, wg.y, wg.z, 0.0f);
-        grad_sum = grad_sum + wg;
-        b.density[i] = rho;
-        b.rho_near[i] = rho_near;
-        const float a = rho / fmaxf(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
-        b.alpha[i] = a;
-        drho += dot(vel, wg);
-        b.kd[i] = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
-        term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
+        term = density_finish(P, b, i, pos, vel, d, found, st->s.dt, solve);
     }
     accumulate_fixed(acc, term);
 }
@@ -943,9 +997,26 @@ inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
 void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n) {
     k_gather<<<blocks_for(n, 256), 256, 0, s>>>(b, n);
 }
+// Shared memory of the staged density_div: nine row starts and `cap` hit
+// codes per thread; caps past 256 take the single-pass kernel.
+size_t density_div_smem(uint32_t cap) {
+    return cap <= 256u ? 9ull * kSolveThreads * 4 + (size_t)cap * kSolveThreads * 2 : 0;
+}
+
+cudaError_t density_div_prepare(uint32_t cap) {
+    const size_t smem = density_div_smem(cap);
+    if (smem > 48 * 1024)
+        return cudaFuncSetAttribute(k_density_div, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return cudaSuccess;
+}
+
 void launch_density_div(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
                         DevSolve *solve, unsigned long long *acc) {
-    k_density_div<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, solve, acc);
+    const size_t smem = density_div_smem(P.nbr_cap);
+    if (smem)
+        k_density_div<<<blocks_for(P.count, kSolveThreads), kSolveThreads, smem, s>>>(P, b, st, solve, acc);
+    else
+        k_density_div_scan<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, solve, acc);
 }
 void launch_div_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
                       unsigned long long *acc) {

@@ -81,6 +81,18 @@ class FluidGrid(C.Structure):
     _fields_ = [("min", C.c_float * 3), ("cell", C.c_float), ("dims", C.c_uint32 * 3)]
 
 
+class FluidMotion(C.Structure):
+    _fields_ = [("gravity", FluidVec3), ("user_acceleration", FluidVec3),
+                ("rotation_rate", FluidVec3)]
+
+
+class FluidFramePlan(C.Structure):
+    _fields_ = [("step", FluidStep), ("force", FluidVec3), ("omega", FluidVec3),
+                ("domega", FluidVec3), ("dt", C.c_float), ("deviation", C.c_float),
+                ("substeps", C.c_uint32), ("refine", C.c_uint32), ("seed", C.c_uint32),
+                ("asleep", C.c_uint32), ("frames", C.c_uint64), ("idle_frames", C.c_uint64)]
+
+
 assert C.sizeof(FluidStep) == 144
 
 
@@ -134,6 +146,20 @@ def lib():
         "fluid_grid_workspace_bytes": (u64, [u32, C.POINTER(FluidGrid)]),
         "fluid_grid_build": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp, u64, vp]),
         "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
+        "fluid_substep_floor": (u32, [f, f]),
+        "fluid_refine_passes": (u32, [f]),
+        "fluid_substeps_for": (u32, [f, f, f, u32]),
+        "fluid_controller_create": (P, [f, C.POINTER(C.c_float * 2), u32]),
+        "fluid_controller_destroy": (None, [P]),
+        "fluid_controller_touch": (i32, [P, u32, f, f, u32]),
+        "fluid_controller_plan": (i32, [P, C.POINTER(FluidMotion), C.c_double, f,
+                                        C.POINTER(FluidFramePlan)]),
+        "fluid_sim_frame_plan": (i32, [P, C.POINTER(FluidFramePlan)]),
+        "fluid_idle_gate_create": (P, []),
+        "fluid_idle_gate_destroy": (None, [P]),
+        "fluid_idle_gate_still_frames": (u32, []),
+        "fluid_idle_gate_asleep": (u32, [P, u32, C.POINTER(C.c_float * 3), f,
+                                         C.POINTER(C.c_float * 3), f]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -245,6 +271,9 @@ class Sim:
         return check(lib().fluid_sim_frame(self.h, v(force), v(omega), v(domega), dt, substeps,
                                            cap, seed), "frame")
 
+    def frame_plan(self, plan):
+        return check(lib().fluid_sim_frame_plan(self.h, C.byref(plan)), "frame_plan")
+
     def sync(self):
         return check(lib().fluid_sim_sync(self.h), "sync")
 
@@ -312,6 +341,39 @@ class Sim:
 
     def stream(self):
         return lib().fluid_sim_stream(self.h)
+
+
+class Controller:
+    """The frame controller of Renderer::frame (render.rs:3021-3098), host only."""
+
+    def __init__(self, spacing, extent, cap=16):
+        ext = (C.c_float * 2)(*[float(v) for v in extent])
+        self.h = lib().fluid_controller_create(spacing, C.byref(ext), cap)
+        if not self.h:
+            raise FluidError(ERR_ARG, "fluid_controller_create")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fluid_controller_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def touch(self, slot, x, y, down):
+        check(lib().fluid_controller_touch(self.h, slot, x, y, 1 if down else 0), "touch")
+
+    def plan(self, gravity, user_acceleration=(0, 0, 0), rotation_rate=(0, 0, 0), now_ms=0.0,
+             v_max=0.0):
+        v = lambda t: FluidVec3(*[float(x) for x in t])
+        m = FluidMotion(v(gravity), v(user_acceleration), v(rotation_rate))
+        out = FluidFramePlan()
+        check(lib().fluid_controller_plan(self.h, C.byref(m), now_ms, v_max, C.byref(out)), "plan")
+        return out
+
+
+def substeps_for(dt, v_max, spacing, cap):
+    return lib().fluid_substeps_for(dt, v_max, spacing, cap)
 
 
 def grid_of(params):

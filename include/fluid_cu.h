@@ -211,6 +211,68 @@ int32_t fluid_sim_advect(FluidSim *sim, const FluidStep *step);
 int32_t fluid_sim_frame(FluidSim *sim, FluidVec3 force, FluidVec3 omega, FluidVec3 domega,
                         float dt, uint32_t substeps, uint32_t cap, uint32_t seed);
 
+/* ---- the frame controller (host only) ------------------------------------ */
+
+/* One reading of the motion sensors, MotionSample (lib.rs:21-37): gravity
+ * and user acceleration in g, device frame; rotation rate in rad/s. */
+typedef struct FluidMotion {
+    FluidVec3 gravity;
+    FluidVec3 user_acceleration;
+    FluidVec3 rotation_rate;
+} FluidMotion;
+
+/* What one frame of Renderer::frame decides before encoding
+ * (render.rs:3021-3098). */
+typedef struct FluidFramePlan {
+    FluidStep step;     /* the Step block each substep runs (dt_sub, v_clamp, fingers) */
+    FluidVec3 force;    /* smoothed body force, m/s^2 */
+    FluidVec3 omega;    /* smoothed angular velocity */
+    FluidVec3 domega;   /* its derivative, clamped to +-200 */
+    float dt;           /* frame dt, clamped to 1/30 s; 0 encodes nothing */
+    float deviation;    /* the force filter's raw-to-smooth deviation */
+    uint32_t substeps;  /* substeps_for on the given v_max; 0 with dt 0 */
+    uint32_t refine;    /* refine_passes(dt / substeps) */
+    uint32_t seed;      /* the frame's tracer seed */
+    uint32_t asleep;    /* 1: the idle gate skipped the frame */
+    uint64_t frames;    /* frames planned (not asleep) */
+    uint64_t idle_frames;
+} FluidFramePlan;
+
+typedef struct FluidController FluidController;
+
+/* render.rs:63-65, :76-78, :97-106: the substep floor, the refine passes of
+ * a substep, and the substep count of a frame. */
+uint32_t fluid_substep_floor(float dt, float dt_sub_max);
+uint32_t fluid_refine_passes(float dt_sub);
+uint32_t fluid_substeps_for(float dt, float v_max, float spacing, uint32_t cap);
+
+/* The controller state Renderer keeps across frames: ForceFilter,
+ * RotationTracker, Fingers, IdleGate (render.rs:862-1105). `extent` is the
+ * box half width and height the fingers map onto; `cap` the substep cap.
+ * Null on bad arguments. */
+FluidController *fluid_controller_create(float spacing, const float extent[2], uint32_t cap);
+void fluid_controller_destroy(FluidController *ctl);
+/* Replaces fluid_renderer_touch (fluid_ffi.h:132-136): slot's finger at
+ * normalised drawable (x, y), or lifted when down is 0. */
+int32_t fluid_controller_touch(FluidController *ctl, uint32_t slot, float x, float y, uint32_t down);
+/* One frame's plan from a motion sample at now_ms (CADisplayLink time) and
+ * the one-frame-stale v_max (FluidSimStats.v_max). */
+int32_t fluid_controller_plan(FluidController *ctl, const FluidMotion *motion, double now_ms,
+                              float v_max, FluidFramePlan *out);
+/* The idle gate alone (IdleGate, render.rs:1024-1105): asleep() is true
+ * while a settled, untouched, unmoved pool's frame may be skipped. */
+typedef struct FluidIdleGate FluidIdleGate;
+FluidIdleGate *fluid_idle_gate_create(void);
+void fluid_idle_gate_destroy(FluidIdleGate *gate);
+uint32_t fluid_idle_gate_still_frames(void);
+uint32_t fluid_idle_gate_asleep(FluidIdleGate *gate, uint32_t touched, const float smooth[3],
+                                float dev, const float omega[3], float v_max);
+
+/* Runs a plan on the GPU (render.rs:3168-3229 minus drawing): its substeps
+ * with its Step block, reduce_stats, and a tracer pass at the frame dt. A
+ * plan that is asleep or has dt 0 encodes nothing. Asynchronous. */
+int32_t fluid_sim_frame_plan(FluidSim *sim, const FluidFramePlan *plan);
+
 /* Waits for the handle's stream. Returns a sticky device error if one was
  * raised (a bounded wait that gave up). */
 int32_t fluid_sim_sync(FluidSim *sim);

@@ -257,3 +257,37 @@ def test_neighbour_overflow_matches_the_oracle(fcu, orc):
         assert_same_bits(sim.field(f), o.field(f), f)
     assert sim.field("counters")[1] > 0
     same_state(sim, o, "overflow")
+
+
+# A neighbour cap past the staged kernel's shared memory takes the
+# single-pass density kernel; the answer is the same.
+def test_a_large_neighbour_cap_matches_the_oracle(fcu, orc):
+    sim, o = pair(fcu, orc, nbr_cap=300)
+    dt = frame_dt(7)
+    s_g, s_o = step_pair(fcu, orc, force=(0.3, -9.81, 0), dt=dt, v_clamp=v_clamp(TB["spacing"], dt))
+    sim.run([s_g] * 5)
+    for _ in range(5):
+        o.substep(s_o)
+    same_state(sim, o, "cap 300")
+
+
+# Collisions: thousands of particles inside one cell (a stencil row longer
+# than the staged kernel's 4,096-slot code span, and more neighbours than
+# the cap) still match the oracle bit for bit.
+def test_a_dense_clump_matches_the_oracle(fcu, orc):
+    cfg = dict(geometry=fcu.GEOMETRY_BOX, box_lo=(0, 0, 0), box_hi=(0.2, 0.2, 0.2), spacing=0.01,
+               h_ratio=1.0, rest_density=1000.0, seeding=fcu.SEED_NONE, count=5000, xsph_blend=0.01)
+    sim, o = pair(fcu, orc, **cfg)
+    rng = np.random.default_rng(11)
+    pos = np.zeros((5000, 4), np.float32)
+    pos[:, :3] = 0.1 + rng.uniform(-0.004, 0.004, (5000, 3))
+    pos[:10, :3] = pos[10, :3]  # exact duplicates: r = 0 pairs
+    sim.set_state(pos4=pos)
+    o.set_state(pos4=pos)
+    dt = float(F32(1.0 / 120.0) / F32(16.0))
+    s_g, s_o = step_pair(fcu, orc, force=(0, -9.81, 0), dt=dt, v_clamp=v_clamp(0.01, dt))
+    sim.step(s_g)
+    o.substep(s_o)
+    for f in ("density", "alpha", "nbr_n", "counters", "kd"):
+        assert_same_bits(sim.field(f), o.field(f), f)
+    same_state(sim, o, "clump")
