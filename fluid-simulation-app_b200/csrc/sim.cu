@@ -584,7 +584,6 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     if ((uint64_t)s->n * cfg->nbr_cap > (1ull << 40)) return fail(FLUID_ERR_ARG, "neighbour lists too large");
 
     CK(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
-    CK(density_div_prepare(cfg->nbr_cap));
     const size_t n = s->n, C = s->cells;
     SimBufs &b = s->b;
     CK(s->alloc(&b.pos, n));

@@ -5,10 +5,11 @@
 // (a million particles fill 148 SMs many times over) and its neighbours are
 // summed in one fixed order: the 27 stencil cells with x fastest, walked as
 // nine rows of three x-adjacent cells, which are one contiguous slot range of
-// the cell-ordered working set; slots ascending. Neighbour lists hold the slot
-// j only (4 bytes, slot-major so a warp's k-th entries are adjacent); the
-// kernel gradient is recomputed from the positions, which do not move inside
-// a substep, bit for bit the value density_div found.
+// the cell-ordered working set; slots ascending. A neighbour list entry is 8
+// bytes, the slot j and the kernel-gradient scale dw / r density_div found
+// (slot-major, so a warp's k-th entries are adjacent); later sweeps form the
+// gradient (dw / r) * (x_i - x_j) from the positions, which do not move
+// inside a substep, bit for bit the value density_div had.
 //
 // Compiled with -fmad=false: no product-sum is fused unless written so.
 #include <cuda_fp16.h>
@@ -399,12 +400,15 @@ __device__ __forceinline__ unsigned long long density_finish(const DevParams &P,
     return fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
 }
 
-// One thread per particle, the scan above: the path for neighbour caps too
-// large for the staged kernel's shared memory.
-__global__ void __launch_bounds__(kSolveThreads) k_density_div_scan(DevParams P, SimBufs b,
-                                                                    const DevStep *__restrict__ st,
-                                                                    DevSolve *solve,
-                                                                    unsigned long long *acc) {
+// One thread per particle over its stencil (sim_solve.wgsl:411-518). A
+// warp-uniform two-phase variant (lanes of one cell row walking the union
+// of their ranges, hits staged in shared memory) was measured slower on the
+// 1M-particle workload (1.39 against 1.29 ms: ~22 instructions per union
+// candidate at 34 % occupancy), so the plain scan stays.
+__global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimBufs b,
+                                                               const DevStep *__restrict__ st,
+                                                               DevSolve *solve,
+                                                               unsigned long long *acc) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     unsigned long long term = 0;
     if (i < P.count) {
@@ -412,100 +416,6 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div_scan(DevParams P,
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         DensitySums d = density_sums_init(P);
         const uint32_t found = density_scan(P, b, i, pos, vel, stencil_of(P, pos), d);
-        term = density_finish(P, b, i, pos, vel, d, found, st->s.dt, solve);
-    }
-    accumulate_fixed(acc, term);
-}
-
-// Two phases. (1) The candidate scan, warp-uniform: lanes whose stencil row
-// is the same cell row walk the union of their slot ranges together, one
-// broadcast load per candidate, each lane keeping its own candidates. A
-// lane's hits go to its own column of shared memory as (row, offset) codes,
-// in row order, slots ascending: the order a per-particle loop finds them.
-// (2) Each lane walks its hits and forms the sums; the lanes advance through
-// their lists together, so the list stores coalesce. A particle with more
-// neighbours than the list holds, or a stencil row longer than 4,096 slots,
-// rescans in phase 2, so its sums still see every neighbour.
-constexpr uint32_t kRowSpan = 4096;  // (row, offset) code: 4 + 12 bits
-
-__global__ void __launch_bounds__(kSolveThreads, 6) k_density_div(DevParams P, SimBufs b,
-                                                                  const DevStep *__restrict__ st,
-                                                                  DevSolve *solve,
-                                                                  unsigned long long *acc) {
-    extern __shared__ uint32_t dyn[];
-    uint32_t *s_row = dyn;                                         // [9][threads]
-    uint16_t *s_hit = reinterpret_cast<uint16_t *>(dyn + 9 * kSolveThreads);  // [cap][threads]
-    const uint32_t n = P.count;
-    const uint32_t tid = threadIdx.x;
-    const uint32_t i = blockIdx.x * blockDim.x + tid;
-    const bool live = i < n;
-    const uint32_t lane = tid & 31;
-    const F3 pos = xyz(__ldg(&b.wpos[live ? i : 0u]));  // lanes past n scan nothing
-    const Stencil t = stencil_of(P, pos);
-    const uint32_t cap = P.nbr_cap;
-    uint32_t found = 0;
-    bool wide = false;
-    int r = 0;
-    for (int oz = -1; oz <= 1; ++oz) {
-        for (int oy = -1; oy <= 1; ++oy, ++r) {
-            uint32_t s = 0, e = 0, rowkey = 0;
-            const bool ok = live && stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey);
-            s_row[r * kSolveThreads + tid] = s;
-            if (ok && e - s > kRowSpan) wide = true;
-            uint32_t pending = __ballot_sync(0xffffffffu, ok);
-            while (pending) {
-                const int leader = __ffs(pending) - 1;
-                const uint32_t lkey = __shfl_sync(0xffffffffu, rowkey, leader);
-                const bool mine = ok && ((pending >> lane) & 1u) && rowkey == lkey;
-                const uint32_t group = __ballot_sync(0xffffffffu, mine);
-                const uint32_t S = __reduce_min_sync(0xffffffffu, mine ? s : 0xffffffffu);
-                const uint32_t E = __reduce_max_sync(0xffffffffu, mine ? e : 0u);
-                for (uint32_t k = S; k < E; ++k) {
-                    const float4 p = __ldg(&b.wpos[k]);
-                    if (mine && k >= s && k < e && k != i) {
-                        const F3 x = pos - xyz(p);
-                        if (dot(x, x) < P.support_sq) {
-                            if (found < cap && !wide)
-                                s_hit[found * kSolveThreads + tid] = (uint16_t)((r << 12) | (k - s));
-                            found++;
-                        }
-                    }
-                }
-                pending &= ~group;
-            }
-        }
-    }
-    unsigned long long term = 0;
-    if (live) {
-        const F3 vel = xyz(__ldg(&b.wvel[i]));
-        DensitySums d = density_sums_init(P);
-        if (found <= cap && !wide) {
-            constexpr int B = 2;
-            for (uint32_t k = 0; k < found; k += B) {
-                uint32_t j[B];
-#pragma unroll
-                for (int u = 0; u < B; ++u) {
-                    const uint32_t code = k + u < found ? s_hit[(k + u) * kSolveThreads + tid] : 0u;
-                    j[u] = k + u < found ? s_row[(code >> 12) * kSolveThreads + tid] + (code & 4095u) : i;
-                }
-                float4 pj[B], vj[B];
-#pragma unroll
-                for (int u = 0; u < B; ++u) {
-                    pj[u] = __ldg(&b.wpos[j[u]]);
-                    vj[u] = __ldg(&b.wvel[j[u]]);
-                }
-#pragma unroll
-                for (int u = 0; u < B; ++u) {
-                    if (k + u < found) {
-                        const F3 x = pos - xyz(pj[u]);
-                        const float gs = density_pair(P, d, pos, vel, x, dot(x, x), vj[u]);
-                        b.nbr[(size_t)(k + u) * n + i] = make_uint2(j[u], __float_as_uint(gs));
-                    }
-                }
-            }
-        } else {
-            found = density_scan(P, b, i, pos, vel, t, d);
-        }
         term = density_finish(P, b, i, pos, vel, d, found, st->s.dt, solve);
     }
     accumulate_fixed(acc, term);
@@ -997,26 +907,9 @@ inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
 void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n) {
     k_gather<<<blocks_for(n, 256), 256, 0, s>>>(b, n);
 }
-// Shared memory of the staged density_div: nine row starts and `cap` hit
-// codes per thread; caps past 256 take the single-pass kernel.
-size_t density_div_smem(uint32_t cap) {
-    return cap <= 256u ? 9ull * kSolveThreads * 4 + (size_t)cap * kSolveThreads * 2 : 0;
-}
-
-cudaError_t density_div_prepare(uint32_t cap) {
-    const size_t smem = density_div_smem(cap);
-    if (smem > 48 * 1024)
-        return cudaFuncSetAttribute(k_density_div, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    return cudaSuccess;
-}
-
 void launch_density_div(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
                         DevSolve *solve, unsigned long long *acc) {
-    const size_t smem = density_div_smem(P.nbr_cap);
-    if (smem)
-        k_density_div<<<blocks_for(P.count, kSolveThreads), kSolveThreads, smem, s>>>(P, b, st, solve, acc);
-    else
-        k_density_div_scan<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, solve, acc);
+    k_density_div<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, solve, acc);
 }
 void launch_div_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
                       unsigned long long *acc) {

@@ -41,9 +41,6 @@ constexpr int kStatsThreads = 256;
 
 // Enqueue helpers: each launches one kernel on `s`.
 void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n);
-// Sets the staged density_div's shared-memory limit for a neighbour cap
-// (once per device, before the first launch or capture).
-cudaError_t density_div_prepare(uint32_t cap);
 void launch_density_div(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
                         DevSolve *solve, unsigned long long *acc);
 void launch_div_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
