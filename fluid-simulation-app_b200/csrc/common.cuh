@@ -68,10 +68,11 @@ struct DevSolve {
     unsigned long long substeps;
     unsigned long long total_div_iters;  // cumulative applies since create
     unsigned long long total_den_iters;
+    uint32_t div_active, den_active;     // the box's tolerance loops go on
     unsigned long long acc_div[kAccSlots];  // fixed-point residual sums (2^-28)
     unsigned long long acc_den[kAccSlots];
 };
-constexpr size_t kSolveHeadBytes = 64;
+constexpr size_t kSolveHeadBytes = 72;
 static_assert(offsetof(DevSolve, acc_div) == kSolveHeadBytes, "DevSolve head");
 
 struct F3 {
@@ -120,6 +121,31 @@ __device__ __forceinline__ unsigned long long warp_sum_u64(unsigned long long v)
 __device__ __forceinline__ void accumulate_fixed(unsigned long long *acc, unsigned long long v) {
     v = warp_sum_u64(v);
     if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
+}
+
+// The same when lanes may add to different accumulators (a warp that
+// straddles two boxes): one atomic per warp when they all share one, one
+// per lane otherwise. Every lane of the warp must call it.
+__device__ __forceinline__ void accumulate_at(unsigned long long *acc, unsigned long long v) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, (unsigned long long)acc);
+    if (peers == 0xffffffffu) {
+        v = warp_sum_u64(v);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(acc, v);
+    } else if (v) {
+        atomicAdd(acc, v);
+    }
+}
+
+// Adds `v` to a per-box 32-bit counter the same way.
+__device__ __forceinline__ void count_at(uint32_t *ctr, uint32_t v) {
+    const uint32_t peers = __match_any_sync(0xffffffffu, (unsigned long long)ctr);
+    if (peers == 0xffffffffu) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(ctr, v);
+    } else if (v) {
+        atomicAdd(ctr, v);
+    }
 }
 
 }  // namespace fcu

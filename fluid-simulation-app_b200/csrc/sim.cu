@@ -89,6 +89,11 @@ void pack_tracer(const float pos[3], float speed, const float e[2], uint32_t out
 
 }  // namespace
 
+namespace fcu {
+// Records an error for fluid_last_error from another translation unit.
+int32_t report_error(int32_t code, const std::string &msg) { return fail(code, msg); }
+}  // namespace fcu
+
 struct FluidSim {
     FluidSimConfig cfg{};
     DevParams P{};
@@ -114,6 +119,21 @@ struct FluidSim {
     cudaEvent_t stats_ready = nullptr;
     bool stats_pending = false;
     float v_max_stale = 0.0f;
+
+    // The sweeps' view of this one-box simulation.
+    Geo geo() const {
+        Geo g{};
+        g.one = P;
+        g.solve = solve;
+        g.st = cur;
+        g.n = n;
+        g.nboxes = 1;
+        return g;
+    }
+    uint32_t stats_chunks() const {
+        const uint32_t c = (n + kStatsThreads - 1) / kStatsThreads;
+        return c < 1u ? 1u : (c > (uint32_t)kStatsChunks ? (uint32_t)kStatsChunks : c);
+    }
 
     template <class T>
     cudaError_t alloc(T **p, size_t count) {
@@ -286,32 +306,33 @@ cudaError_t enqueue_substep(FluidSim *s, cudaStream_t st, uint32_t div_iters, ui
                            true, s->ring, s->cur, s->solve, kRing);
     if (e != cudaSuccess) return e;
     mark("grid");
+    const Geo g = s->geo();
     launch_gather(st, s->b, s->n);
     mark("gather");
-    launch_density_div(st, s->P, s->b, s->cur, s->solve, &s->solve->acc_div[0]);
+    launch_density_div(st, g, s->b, 0);
     mark("density_div");
     if (density_only) return cudaGetLastError();
     for (uint32_t d = 0; d < div_iters; ++d) {
         if (d > 0) {
-            launch_div_kappa(st, s->P, s->b, s->cur, &s->solve->acc_div[d]);
+            launch_div_kappa(st, g, s->b, (int)d, kGateNone);
             mark("div_kappa");
         }
-        launch_apply(st, s->P, s->b, s->cur, false);
+        launch_apply(st, g, s->b, false, kGateNone);
         mark("div_apply");
     }
-    launch_forces_eval(st, s->P, s->b);
+    launch_forces_eval(st, g, s->b);
     mark("forces_eval");
-    launch_forces_apply(st, s->P, s->b, s->cur);
+    launch_forces_apply(st, g, s->b);
     mark("forces_den_apply");
     for (uint32_t k = 0; k < den_iters; ++k) {
-        launch_den_kappa(st, s->P, s->b, s->cur, &s->solve->acc_den[k]);
+        launch_den_kappa(st, g, s->b, (int)k, kGateNone);
         mark("den_kappa");
-        launch_apply(st, s->P, s->b, s->cur, true);
+        launch_apply(st, g, s->b, true, kGateNone);
         mark("den_apply");
     }
     const int div_slot = div_iters > 0 ? (int)div_iters - 1 : 0;
-    launch_integrate(st, s->P, s->b, s->cur, s->solve, div_slot, den_iters > 0 ? (int)den_iters - 1 : -1,
-                     (int)div_iters, (int)den_iters);
+    launch_integrate(st, g, s->b, div_slot, den_iters > 0 ? (int)den_iters - 1 : -1, (int)div_iters,
+                     (int)den_iters);
     mark("integrate");
     return cudaGetLastError();
 }
@@ -379,21 +400,21 @@ int32_t capture_tolerance(FluidSim *s, cudaGraphExec_t *out) {
     if (e == cudaSuccess)
         e = grid_build_enqueue(st, s->b.pos, s->n, geom_of(s->P), s->b.keys, s->b.starts, s->b.perm, s->gw,
                                true, s->ring, s->cur, s->solve, kRing);
+    const Geo geo = s->geo();
     if (e == cudaSuccess) {
         launch_gather(st, s->b, s->n);
-        launch_density_div(st, s->P, s->b, s->cur, s->solve, &s->solve->acc_div[0]);
-        launch_tol_finish(st, s->solve, s->n, 0, 1, c.div_tol, c.max_iters, hdiv);
+        launch_density_div(st, geo, s->b, 0);
+        launch_tol_finish(st, geo, 0, 1, c.div_tol, c.max_iters, hdiv);
         rc = add_while(st, g, hdiv, &bdiv);
     }
     if (e == cudaSuccess && rc == FLUID_OK) {
-        launch_forces_eval(st, s->P, s->b);
-        launch_forces_apply(st, s->P, s->b, s->cur);
-        launch_den_kappa(st, s->P, s->b, s->cur, &s->solve->acc_den[0]);
-        launch_tol_finish(st, s->solve, s->n, 1, 1, c.den_tol, c.max_iters, hden);
+        launch_forces_eval(st, geo, s->b);
+        launch_forces_apply(st, geo, s->b);
+        launch_den_kappa(st, geo, s->b, 0, kGateNone);
+        launch_tol_finish(st, geo, 1, 1, c.den_tol, c.max_iters, hden);
         rc = add_while(st, g, hden, &bden);
     }
-    if (e == cudaSuccess && rc == FLUID_OK)
-        launch_integrate(st, s->P, s->b, s->cur, s->solve, -1, -1, 0, 0);
+    if (e == cudaSuccess && rc == FLUID_OK) launch_integrate(st, geo, s->b, -1, -1, 0, 0);
     if (e == cudaSuccess) e = cudaGetLastError();
     cudaGraph_t g2 = nullptr;
     cudaError_t e2 = cudaStreamEndCapture(st, &g2);
@@ -405,14 +426,14 @@ int32_t capture_tolerance(FluidSim *s, cudaGraphExec_t *out) {
     }
     // loop bodies
     CK(cudaStreamBeginCaptureToGraph(s->side, bdiv, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    launch_apply(s->side, s->P, s->b, s->cur, false);
-    launch_div_kappa(s->side, s->P, s->b, s->cur, &s->solve->acc_div[0]);
-    launch_tol_finish(s->side, s->solve, s->n, 0, 0, c.div_tol, c.max_iters, hdiv);
+    launch_apply(s->side, geo, s->b, false, kGateDiv);
+    launch_div_kappa(s->side, geo, s->b, 0, kGateDiv);
+    launch_tol_finish(s->side, geo, 0, 0, c.div_tol, c.max_iters, hdiv);
     CK(cudaStreamEndCapture(s->side, &bdiv));
     CK(cudaStreamBeginCaptureToGraph(s->side, bden, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    launch_apply(s->side, s->P, s->b, s->cur, true);
-    launch_den_kappa(s->side, s->P, s->b, s->cur, &s->solve->acc_den[0]);
-    launch_tol_finish(s->side, s->solve, s->n, 1, 0, c.den_tol, c.max_iters, hden);
+    launch_apply(s->side, geo, s->b, true, kGateDen);
+    launch_den_kappa(s->side, geo, s->b, 0, kGateDen);
+    launch_tol_finish(s->side, geo, 1, 0, c.den_tol, c.max_iters, hden);
     CK(cudaStreamEndCapture(s->side, &bden));
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
@@ -469,7 +490,7 @@ int32_t run_frame(FluidSim *s, const FluidStep &st, uint32_t n, uint32_t refine,
     rc = substep_graph(s, refine, &g);
     if (rc != FLUID_OK) return rc;
     for (uint32_t k = 0; k < n; ++k) CK(cudaGraphLaunch(g, s->stream));
-    launch_stats(s->stream, s->P, s->b, s->solve);
+    launch_stats(s->stream, s->geo(), s->b, s->stats_chunks());
     if (s->ntr) {
         FluidStep tr;
         std::memset(&tr, 0, sizeof tr);
@@ -615,7 +636,7 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(s->alloc(&b.tracers, 2 * (size_t)(s->ntr > 0 ? s->ntr : 1)));
     CK(s->alloc(&b.vel_grid, 4 * C));
     CK(s->alloc(&b.vel_flat, C));
-    CK(s->alloc(&b.stats_part, (size_t)kStatsBlocks * 12));
+    CK(s->alloc(&b.stats_part, (size_t)kStatsChunks * 12));
     CK(s->alloc(&b.stats_acc, 1));
     CK(s->alloc(&b.stats, 16));
     CK(s->alloc(&s->ring, kRing));
@@ -721,7 +742,7 @@ int32_t fluid_sim_step(FluidSim *s, const FluidStep *step) { return fluid_sim_ru
 int32_t fluid_sim_reduce_stats(FluidSim *s) {
     if (!s) return fail(FLUID_ERR_ARG, "null handle");
     CK(cudaSetDevice(s->device));
-    launch_stats(s->stream, s->P, s->b, s->solve);
+    launch_stats(s->stream, s->geo(), s->b, s->stats_chunks());
     CK(cudaGetLastError());
     return FLUID_OK;
 }

@@ -260,6 +260,34 @@ __global__ void __launch_bounds__(256) k_gather(SimBufs b, uint32_t n) {
     b.wid[k] = __ldg(&b.id[i]);
 }
 
+// Per-box views of a Geo. kB (batch) is a template flag so the one-box
+// kernels keep their constants in parameter space and their sums on the
+// plain warp-aggregated atomics.
+template <bool kB>
+__device__ __forceinline__ uint32_t box_index(const Geo &g, uint32_t i) {
+    return kB ? (uint32_t)__ldg(&g.box_of[i]) : 0u;
+}
+template <bool kB>
+__device__ __forceinline__ DevParams params_of(const Geo &g, uint32_t bi) {
+    if (kB) return g.box[bi];
+    return g.one;
+}
+template <bool kB>
+__device__ __forceinline__ uint32_t cell_base_of(const Geo &g, uint32_t bi) {
+    return kB ? __ldg(&g.cell_base[bi]) : 0u;
+}
+template <bool kB>
+__device__ __forceinline__ uint32_t first_of(const Geo &g, uint32_t bi) {
+    return kB ? __ldg(&g.first[bi]) : 0u;
+}
+// Adds a thread's fixed-point term to its box's accumulator; every lane of
+// the warp calls it.
+template <bool kB>
+__device__ __forceinline__ void add_term(unsigned long long *acc, unsigned long long v) {
+    if (kB) accumulate_at(acc, v);
+    else accumulate_fixed(acc, v);
+}
+
 // One row (oz, oy) of a particle's 27-cell stencil: three x-adjacent cells,
 // one contiguous slot range of the cell-ordered working set. Cell culling: a
 // stencil cell whose nearest point lies beyond the support holds no
@@ -291,9 +319,10 @@ __device__ __forceinline__ Stencil stencil_of(const DevParams &P, F3 pos) {
     return t;
 }
 
-__device__ __forceinline__ bool stencil_row(const DevParams &P, const uint32_t *__restrict__ starts,
-                                            uint32_t n, const Stencil &t, int oz, int oy,
-                                            uint32_t &s, uint32_t &e, uint32_t &rowkey) {
+__device__ __forceinline__ bool stencil_row(const DevParams &P, uint32_t cell_base,
+                                            const uint32_t *__restrict__ starts, uint32_t n,
+                                            const Stencil &t, int oz, int oy, uint32_t &s,
+                                            uint32_t &e) {
     const int cz = t.bz + oz, cy = t.by + oy;
     if (cz < 0 || cz >= (int)P.dims[2] || cy < 0 || cy >= (int)P.dims[1]) return false;
     const float dzp = oz < 0 ? t.zl * t.zl : (oz > 0 ? t.zh * t.zh : 0.0f);
@@ -301,9 +330,9 @@ __device__ __forceinline__ bool stencil_row(const DevParams &P, const uint32_t *
     if (dperp >= P.support_sq) return false;
     const int cx0 = (t.bx > 0 && dperp + t.xl * t.xl < P.support_sq) ? t.bx - 1 : t.bx;
     const int cx1 = (t.bx + 1 < (int)P.dims[0] && dperp + t.xh * t.xh < P.support_sq) ? t.bx + 1 : t.bx;
-    rowkey = ((uint32_t)cz * P.dims[1] + (uint32_t)cy) * P.dims[0];
-    s = __ldg(&starts[rowkey + cx0]);
-    e = __ldg(&starts[rowkey + cx1 + 1]);
+    const uint32_t row = cell_base + ((uint32_t)cz * P.dims[1] + (uint32_t)cy) * P.dims[0];
+    s = __ldg(&starts[row + cx0]);
+    e = __ldg(&starts[row + cx1 + 1]);
     if (e > n) e = n;  // starts never exceed n unless a scan gave up
     return s < e;
 }
@@ -330,106 +359,101 @@ __device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d
 }
 
 // ---- density_div (sim_solve.wgsl:411-518) --------------------------------
-
-// The single-pass scan: every candidate of the stencil, in order, each hit
-// summed and listed (the first `cap` of them). Returns the hits found.
-__device__ __forceinline__ uint32_t density_scan(const DevParams &P, const SimBufs &b, uint32_t i,
-                                                 F3 pos, F3 vel, const Stencil &t, DensitySums &d) {
-    const uint32_t n = P.count, cap = P.nbr_cap;
-    uint32_t seen = 0;
-    for (int oz = -1; oz <= 1; ++oz)
-        for (int oy = -1; oy <= 1; ++oy) {
-            uint32_t s, e, rowkey;
-            if (!stencil_row(P, b.starts, n, t, oz, oy, s, e, rowkey)) continue;
-            for (uint32_t k = s; k < e; ++k) {
-                if (k == i) continue;
-                const F3 x = pos - xyz(__ldg(&b.wpos[k]));
-                const float r2 = dot(x, x);
-                if (r2 >= P.support_sq) continue;
-                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
-                if (seen < cap) b.nbr[(size_t)seen * n + i] = make_uint2(k, __float_as_uint(gs));
-                seen++;
-            }
-        }
-    return seen;
-}
-
-__device__ __forceinline__ DensitySums density_sums_init(const DevParams &P) {
-    DensitySums d;
-    d.w_sum = P.sigma;  // lane 0's self term W(0), sim_solve.wgsl:426
-    d.rho_near = 0.0f;
-    d.grad_sq = 0.0f;
-    d.drho = 0.0f;
-    d.grad_sum = f3(0.f, 0.f, 0.f);
-    return d;
-}
-
-// Everything density_div does after its neighbour sums (sim_solve.wgsl:
-// 475-517): list length and overflow, density with the wall fill, the wall
-// gradient, alpha, the divergence kappa; returns the residual term.
-__device__ __forceinline__ unsigned long long density_finish(const DevParams &P, const SimBufs &b,
-                                                             uint32_t i, F3 pos, F3 vel,
-                                                             const DensitySums &d, uint32_t found,
-                                                             float dt, DevSolve *solve) {
-    const uint32_t cap = P.nbr_cap;
-    b.nbr_n[i] = found < cap ? found : cap;
-    if (found > cap) atomicAdd(&solve->nbr_over, found - cap);
-    float rho = P.mass * d.w_sum;
-    const float rho_near = d.rho_near;
-    const float grad_sq = P.mass * P.mass * d.grad_sq;
-    float drho = P.mass * d.drho;
-    F3 grad_sum = P.mass * d.grad_sum;
-    const F3 lo = wall_lo(P), hi = wall_hi(P);
-    const F3 tl = (pos - lo) * P.inv_h;
-    const F3 th = (hi - pos) * P.inv_h;
-    float fill = 0.0f;
-    fill += wall_density(tl.x) + wall_density(th.x);
-    fill += wall_density(tl.y) + wall_density(th.y);
-    fill += wall_density(tl.z) + wall_density(th.z);
-    fill -= wedge_sum(tl, th);
-    rho += P.rho0 * fill;
-    const F3 wg = wall_grad_sum(P, pos);
-    b.wgrad[i] = make_float4(wg.x, wg.y, wg.z, 0.0f);
-    grad_sum = grad_sum + wg;
-    b.density[i] = rho;
-    b.rho_near[i] = rho_near;
-    const float a = rho / fmaxf(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
-    b.alpha[i] = a;
-    drho += dot(vel, wg);
-    b.kd[i] = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
-    return fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
-}
-
-// One thread per particle over its stencil (sim_solve.wgsl:411-518). A
-// warp-uniform two-phase variant (lanes of one cell row walking the union
-// of their ranges, hits staged in shared memory) was measured slower on the
-// 1M-particle workload (1.39 against 1.29 ms: ~22 instructions per union
-// candidate at 34 % occupancy), so the plain scan stays.
-__global__ void __launch_bounds__(kSolveThreads) k_density_div(DevParams P, SimBufs b,
-                                                               const DevStep *__restrict__ st,
-                                                               DevSolve *solve,
-                                                               unsigned long long *acc) {
+// One thread per particle over its stencil. A warp-uniform two-phase variant
+// (lanes of one cell row walking the union of their ranges, hits staged in
+// shared memory) was measured slower on the 1M-particle workload (1.39
+// against 1.29 ms: ~22 instructions per union candidate at 34 % occupancy),
+// so the plain scan stays. Every candidate of the stencil is taken in order;
+// each hit is summed and the first `cap` are listed.
+template <bool kB>
+__global__ void __launch_bounds__(kSolveThreads) k_density_div(Geo g, SimBufs b, int slot) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
-    if (i < P.count) {
+    if (live) {
+        const DevParams P = params_of<kB>(g, bi);
+        const uint32_t base = cell_base_of<kB>(g, bi);
+        const float dt = g.st[bi].s.dt;
         const F3 pos = xyz(__ldg(&b.wpos[i]));
         const F3 vel = xyz(__ldg(&b.wvel[i]));
-        DensitySums d = density_sums_init(P);
-        const uint32_t found = density_scan(P, b, i, pos, vel, stencil_of(P, pos), d);
-        term = density_finish(P, b, i, pos, vel, d, found, st->s.dt, solve);
+        const Stencil t = stencil_of(P, pos);
+        const uint32_t cap = P.nbr_cap;
+        DensitySums d;
+        d.w_sum = P.sigma;  // lane 0's self term W(0), sim_solve.wgsl:426
+        d.rho_near = 0.0f;
+        d.grad_sq = 0.0f;
+        d.drho = 0.0f;
+        d.grad_sum = f3(0.f, 0.f, 0.f);
+        uint32_t found = 0;
+        for (int oz = -1; oz <= 1; ++oz)
+            for (int oy = -1; oy <= 1; ++oy) {
+                uint32_t s, e;
+                if (!stencil_row(P, base, b.starts, n, t, oz, oy, s, e)) continue;
+                for (uint32_t k = s; k < e; ++k) {
+                    if (k == i) continue;
+                    const F3 x = pos - xyz(__ldg(&b.wpos[k]));
+                    const float r2 = dot(x, x);
+                    if (r2 >= P.support_sq) continue;
+                    const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
+                    if (found < cap) b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
+                    found++;
+                }
+            }
+        // sim_solve.wgsl:475-517
+        b.nbr_n[i] = found < cap ? found : cap;
+        if (found > cap) atomicAdd(&g.solve[bi].nbr_over, found - cap);
+        float rho = P.mass * d.w_sum;
+        const float rho_near = d.rho_near;
+        const float grad_sq = P.mass * P.mass * d.grad_sq;
+        float drho = P.mass * d.drho;
+        F3 grad_sum = P.mass * d.grad_sum;
+        const F3 lo = wall_lo(P), hi = wall_hi(P);
+        const F3 tl = (pos - lo) * P.inv_h;
+        const F3 th = (hi - pos) * P.inv_h;
+        float fill = 0.0f;
+        fill += wall_density(tl.x) + wall_density(th.x);
+        fill += wall_density(tl.y) + wall_density(th.y);
+        fill += wall_density(tl.z) + wall_density(th.z);
+        fill -= wedge_sum(tl, th);
+        rho += P.rho0 * fill;
+        const F3 wg = wall_grad_sum(P, pos);
+        b.wgrad[i] = make_float4(wg.x, wg.y, wg.z, 0.0f);
+        grad_sum = grad_sum + wg;
+        b.density[i] = rho;
+        b.rho_near[i] = rho_near;
+        const float a = rho / fmaxf(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
+        b.alpha[i] = a;
+        drho += dot(vel, wg);
+        b.kd[i] = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
+        term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
     }
-    accumulate_fixed(acc, term);
+    add_term<kB>(&g.solve[bi].acc_div[slot], term);
+}
+
+// Whether box bi's tolerance loop `gate` has stopped (its kernels skip it).
+template <bool kB>
+__device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
+    if (!kB || gate == kGateNone) return false;
+    const DevSolve &sv = g.solve[bi];
+    return (gate == kGateDiv ? sv.div_active : sv.den_active) == 0u;
 }
 
 // ---- divergence predictor for a later divergence iteration ---------------
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(DevParams P, SimBufs b,
-                                                             const DevStep *__restrict__ st,
-                                                             unsigned long long *acc) {
-    const uint32_t n = P.count;
+// density_div's divergence sums again over the list, with this
+// iteration's velocities.
+template <bool kB>
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(Geo g, SimBufs b, int slot,
+                                                                       int gate) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float dt = st->s.dt;
+    const bool live = i < n;
+    const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
-    if (i < n) {
+    if (live && !gated_out<kB>(g, bi, gate)) {
+        const DevParams P = params_of<kB>(g, bi);
+        const float dt = g.st[bi].s.dt;
         const F3 pos = xyz(__ldg(&b.wpos[i]));
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
@@ -444,12 +468,11 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(DevParams
         b.kd[i] = fmaxf(drho, 0.0f) * __ldg(&b.alpha[i]) / fmaxf(dt, 1e-9f) / rho;
         term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
     }
-    accumulate_fixed(acc, term);
+    add_term<kB>(&g.solve[bi].acc_div[slot], term);
 }
 
 // kappa_partial (sim_solve.wgsl:596-606), sequential over the list.
-__device__ __forceinline__ F3 kappa_sum(const DevParams &P, const SimBufs &b, uint32_t i,
-                                        uint32_t n, F3 pos, float kd_i) {
+__device__ __forceinline__ F3 kappa_sum(const SimBufs &b, uint32_t i, uint32_t n, F3 pos, float kd_i) {
     const uint32_t cnt = __ldg(&b.nbr_n[i]);
     F3 dv = f3(0.f, 0.f, 0.f);
     walk<FCU_B_KD, PosKd>(
@@ -461,17 +484,20 @@ __device__ __forceinline__ F3 kappa_sum(const DevParams &P, const SimBufs &b, ui
 // ---- apply_kappa_wide: div_apply / den_apply (sim_solve.wgsl:608-621) -----
 // For the density iterations the applied pressure k*rho that den_kappa held
 // back joins the pressure here, with the kappa it belongs to.
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_apply(DevParams P, SimBufs b,
-                                                         const DevStep *__restrict__ st,
-                                                         int add_pressure) {
-    const uint32_t n = P.count;
+template <bool kB>
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure,
+                                                                   int gate) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float dt = st->s.dt;
+    const uint32_t bi = box_index<kB>(g, i);
+    if (gated_out<kB>(g, bi, gate)) return;
+    const float mass = params_of<kB>(g, bi).mass;
+    const float dt = g.st[bi].s.dt;
     const F3 pos = xyz(__ldg(&b.wpos[i]));
     const float kd_i = b.kd[i];
-    const F3 total = kappa_sum(P, b, i, n, pos, kd_i);
-    const F3 dv_full = P.mass * total + kd_i * xyz(__ldg(&b.wgrad[i]));
+    const F3 total = kappa_sum(b, i, n, pos, kd_i);
+    const F3 dv_full = mass * total + kd_i * xyz(__ldg(&b.wgrad[i]));
     const float4 was = b.wvel[i];
     const F3 v = xyz(was) - dt * dv_full;
     b.wvel[i] = make_float4(v.x, v.y, v.z, was.w);
@@ -479,10 +505,12 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_apply(DevParams P, 
 }
 
 // ---- forces_eval (sim_solve.wgsl:524-592) ---------------------------------
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_eval(DevParams P, SimBufs b) {
-    const uint32_t n = P.count;
+template <bool kB>
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_eval(Geo g, SimBufs b) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const DevParams P = params_of<kB>(g, box_index<kB>(g, i));
     const float coh_c = 2.0f * P.h;
     const float c3 = coh_c * coh_c * coh_c;
     const float coh_k = 32.0f / (3.14159265f * c3 * c3 * c3);
@@ -557,16 +585,19 @@ __device__ __forceinline__ F3 fingers(const FluidStep &st, F3 pos, F3 v) {
 }
 
 // ---- forces_den_apply (sim_solve.wgsl:630-663) -----------------------------
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_apply(DevParams P, SimBufs b,
-                                                                const DevStep *__restrict__ stp) {
-    const uint32_t n = P.count;
+template <bool kB>
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_apply(Geo g, SimBufs b) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const uint32_t bi = box_index<kB>(g, i);
+    const float mass = params_of<kB>(g, bi).mass;
+    const DevStep *stp = &g.st[bi];
     const FluidStep &st = stp->s;
     const float dt = st.dt;
     const F3 pos = xyz(__ldg(&b.wpos[i]));
     const float kd_i = b.kd[i];
-    const F3 total = kappa_sum(P, b, i, n, pos, kd_i);
+    const F3 total = kappa_sum(b, i, n, pos, kd_i);
     const float4 a = __ldg(&b.accel[i]);
     const F3 r = pos;
     const float4 was = b.wvel[i];
@@ -577,20 +608,24 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_apply(DevPar
     const F3 fict = -cross(domega, r) - cross(omega, cross(omega, r)) - 2.0f * cross(omega, v);
     const F3 forced = fingers(st, r, v + dt * (force + fict + xyz(a)) + stp->xsph_blend * xyz(__ldg(&b.xsph[i])));
     b.wtemp[i] += dt * a.w;
-    const F3 dv_full = P.mass * total + kd_i * xyz(__ldg(&b.wgrad[i]));
+    const F3 dv_full = mass * total + kd_i * xyz(__ldg(&b.wgrad[i]));
     const F3 o = forced - dt * dv_full;
     b.wvel[i] = make_float4(o.x, o.y, o.z, was.w);
 }
 
 // ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(DevParams P, SimBufs b,
-                                                             const DevStep *__restrict__ st,
-                                                             unsigned long long *acc) {
-    const uint32_t n = P.count;
+template <bool kB>
+__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(Geo g, SimBufs b, int slot,
+                                                                       int gate) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float dt = st->s.dt;
+    const bool live = i < n;
+    const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
-    if (i < n) {
+    if (live && !gated_out<kB>(g, bi, gate)) {
+        const DevParams P = params_of<kB>(g, bi);
+        const float mass = P.mass, rho0 = P.rho0;
+        const float dt = g.st[bi].s.dt;
         const F3 pos = xyz(__ldg(&b.wpos[i]));
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
@@ -600,29 +635,32 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(DevParams
             [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
             [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
         const float rho = __ldg(&b.density[i]);
-        drho = P.mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
+        drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;
-        const float kk = fmaxf(rho_star - P.rho0, 0.0f) * __ldg(&b.alpha[i]) / (dt * dt);
+        const float kk = fmaxf(rho_star - rho0, 0.0f) * __ldg(&b.alpha[i]) / (dt * dt);
         b.kd[i] = kk / rho;
         b.pinc[i] = kk * rho;
-        term = fixed_term((double)rho_star / (double)P.rho0 - 1.0);
+        term = fixed_term((double)rho_star / (double)rho0 - 1.0);
     }
-    accumulate_fixed(acc, term);
+    add_term<kB>(&g.solve[bi].acc_den[slot], term);
 }
 
 // ---- integrate (sim_solve.wgsl:709-756) ------------------------------------
-// With div_slot >= 0 (the fixed schedule) thread 0 also records the
-// substep's residuals from the accumulator slots of the last divergence and
+// With div_slot >= 0 (the fixed schedule) each box's first slot also records
+// the box's residuals from the accumulator slots of the last divergence and
 // density predictions, and the iteration counts.
-__global__ void __launch_bounds__(256) k_integrate(DevParams P, SimBufs b,
-                                                   const DevStep *__restrict__ stp, DevSolve *solve,
-                                                   int div_slot, int den_slot, int div_iters,
-                                                   int den_iters) {
-    const uint32_t n = P.count;
+template <bool kB>
+__global__ void __launch_bounds__(256) k_integrate(Geo g, SimBufs b, int div_slot, int den_slot,
+                                                   int div_iters, int den_iters) {
+    const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const FluidStep &st = stp->s;
-    bool clamped_speed = false;
-    if (i < n) {
+    const bool live = i < n;
+    const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
+    uint32_t clamped_speed = 0;
+    if (live) {
+        const DevParams P = params_of<kB>(g, bi);
+        const DevStep *stp = &g.st[bi];
+        const FluidStep &st = stp->s;
         const float4 was = __ldg(&b.wvel[i]);
         F3 v = xyz(was);
         const float speed = len(v);
@@ -630,7 +668,7 @@ __global__ void __launch_bounds__(256) k_integrate(DevParams P, SimBufs b,
         const float ceiling = rho < 0.5f * P.rho0 ? 3.0f * st.v_clamp : st.v_clamp;
         if (speed > ceiling) {
             v = v * (ceiling / speed);
-            clamped_speed = true;
+            clamped_speed = 1;
         }
         const float4 pv = __ldg(&b.wpvel[i]);
         const float accel = len(v - xyz(pv)) / st.dt;
@@ -650,60 +688,83 @@ __global__ void __launch_bounds__(256) k_integrate(DevParams P, SimBufs b,
         const float t = __ldg(&b.wtemp[i]);
         b.temp[i] = t + t * EXPANSION / (rho * HEAT_CAPACITY) * dp;
         b.id[i] = __ldg(&b.wid[i]);
-    }
-    const uint32_t m = __ballot_sync(0xffffffffu, clamped_speed);
-    if ((threadIdx.x & 31) == 0 && m) atomicAdd(&solve->clamp_count, __popc(m));
-    if (i == 0) {
-        solve->substeps += 1ull;
-        if (div_slot >= 0) {
-            solve->div_res = (double)solve->acc_div[div_slot] / kFixedScale / (double)n;
-            solve->den_res =
-                den_slot >= 0 ? (double)solve->acc_den[den_slot] / kFixedScale / (double)n : 0.0;
-            solve->div_iters = (uint32_t)div_iters;
-            solve->den_iters = (uint32_t)den_iters;
-            solve->total_div_iters += (unsigned long long)div_iters;
-            solve->total_den_iters += (unsigned long long)den_iters;
+        if (i == first_of<kB>(g, bi)) {
+            DevSolve *sv = &g.solve[bi];
+            const double nb = (double)P.count;
+            sv->substeps += 1ull;
+            if (div_slot >= 0) {
+                sv->div_res = (double)sv->acc_div[div_slot] / kFixedScale / nb;
+                sv->den_res = den_slot >= 0 ? (double)sv->acc_den[den_slot] / kFixedScale / nb : 0.0;
+                sv->div_iters = (uint32_t)div_iters;
+                sv->den_iters = (uint32_t)den_iters;
+                sv->total_div_iters += (unsigned long long)div_iters;
+                sv->total_den_iters += (unsigned long long)den_iters;
+            }
         }
+    }
+    if (kB) {
+        count_at(&g.solve[bi].clamp_count, clamped_speed);
+    } else {
+        const uint32_t m = __ballot_sync(0xffffffffu, clamped_speed != 0u);
+        if ((threadIdx.x & 31) == 0 && m) atomicAdd(&g.solve[0].clamp_count, __popc(m));
     }
 }
 
-// The tolerance loop's bookkeeping (one thread): reads and clears the
-// residual accumulator of `which` (0 divergence, 1 density), counts the
-// iteration unless `first`, records the residual, and sets the graph's
-// loop condition: go on while under max_iters and the residual is above
-// tol (the divergence loop always makes its first apply, as the reference).
-__global__ void k_tol_finish(DevSolve *solve, uint32_t n, int which, int first, float tol,
-                             uint32_t max_iters, cudaGraphConditionalHandle handle) {
-    unsigned long long *acc = which == 0 ? &solve->acc_div[0] : &solve->acc_den[0];
-    const double res = (double)*acc / kFixedScale / (double)n;
-    *acc = 0ull;
-    uint32_t *iters = which == 0 ? &solve->div_iters : &solve->den_iters;
-    const uint32_t it = first ? 0u : *iters + 1u;
-    *iters = it;
-    if (!first) {
-        if (which == 0) solve->total_div_iters += 1ull;
-        else solve->total_den_iters += 1ull;
+// The tolerance loops' bookkeeping, one block over the boxes: for each box
+// whose loop runs (every box on the first call), read and clear its
+// residual accumulator of `which` (0 divergence, 1 density), count the
+// iteration unless `first`, record the residual, and go on while under
+// max_iters and above tol (the divergence loop always makes its first
+// apply, as the reference). The graph's loop continues while any box does.
+__global__ void __launch_bounds__(256) k_tol_finish(Geo g, int which, int first, float tol,
+                                                    uint32_t max_iters,
+                                                    cudaGraphConditionalHandle handle) {
+    int any = 0;
+    for (uint32_t bi = threadIdx.x; bi < g.nboxes; bi += blockDim.x) {
+        DevSolve *sv = &g.solve[bi];
+        uint32_t *active = which == 0 ? &sv->div_active : &sv->den_active;
+        if (!first && !*active) continue;
+        unsigned long long *acc = which == 0 ? &sv->acc_div[0] : &sv->acc_den[0];
+        const uint32_t cnt = g.box_of ? g.box[bi].count : g.one.count;
+        const double res = (double)*acc / kFixedScale / (double)cnt;
+        *acc = 0ull;
+        uint32_t *iters = which == 0 ? &sv->div_iters : &sv->den_iters;
+        const uint32_t it = first ? 0u : *iters + 1u;
+        *iters = it;
+        if (!first) {
+            if (which == 0) sv->total_div_iters += 1ull;
+            else sv->total_den_iters += 1ull;
+        }
+        if (which == 0) sv->div_res = res;
+        else sv->den_res = res;
+        const bool go = it < max_iters && (res > (double)tol || (which == 0 && it < 1u));
+        *active = go ? 1u : 0u;
+        any |= go ? 1 : 0;
     }
-    if (which == 0) solve->div_res = res;
-    else solve->den_res = res;
-    const bool go = it < max_iters && (res > (double)tol || (which == 0 && it < 1u));
-    cudaGraphSetConditional(handle, go ? 1u : 0u);
+    any = __syncthreads_or(any);
+    if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
 }
 
 // ---- reduce_stats (sim_solve.wgsl:800-874) ---------------------------------
-// Per-block partials, then one block folds them; min and max are exact in
-// any order and the compression sum is an integer sum.
-__global__ void __launch_bounds__(kStatsThreads) k_stats_partial(DevParams P, SimBufs b) {
-    const uint32_t n = P.count;
+// Per box, per-chunk partials (block (chunk, box) strides through the box's
+// slots), then one thread per box folds them; min and max are exact in any
+// order and the compression sum is an integer sum.
+template <bool kB>
+__global__ void __launch_bounds__(kStatsThreads) k_stats_partial(Geo g, SimBufs b) {
+    const uint32_t bi = blockIdx.y;
+    const DevParams P = params_of<kB>(g, bi);
+    const uint32_t first = first_of<kB>(g, bi);
+    const uint32_t end = first + P.count;
     __shared__ float sh[12][kStatsThreads / 32];
     __shared__ unsigned long long ssum[kStatsThreads / 32];
     float m = 0.0f, lo = HUGE_F, hi = -HUGE_F;
     float v_lo = HUGE_F, v_hi = -HUGE_F, a_lo = HUGE_F, a_hi = -HUGE_F;
     float p_lo = HUGE_F, p_hi = -HUGE_F, t_lo = HUGE_F, t_hi = -HUGE_F;
     unsigned long long sum = 0;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float rho0 = P.rho0;
+    for (uint32_t i = first + blockIdx.x * blockDim.x + threadIdx.x; i < end; i += gridDim.x * blockDim.x) {
         const float d = __ldg(&b.density[i]);
-        const float c = d / P.rho0 - 1.0f;
+        const float c = d / rho0 - 1.0f;
         sum += fixed_term((double)fmaxf(c, 0.0f));
         m = fmaxf(m, c);
         lo = fminf(lo, d);
@@ -747,24 +808,28 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats_partial(DevParams P, Si
             for (int q = 0; q < 11; ++q) out[q] = is_max[q] ? fmaxf(out[q], sh[q][w]) : fminf(out[q], sh[q][w]);
             s += ssum[w];
         }
-        for (int q = 0; q < 11; ++q) b.stats_part[blockIdx.x * 12 + q] = out[q];
-        atomicAdd(b.stats_acc, s);
+        float *part = b.stats_part + ((size_t)bi * gridDim.x + blockIdx.x) * 12;
+        for (int q = 0; q < 11; ++q) part[q] = out[q];
+        atomicAdd(&b.stats_acc[bi], s);
     }
 }
 
-__global__ void k_stats_final(DevParams P, SimBufs b, DevSolve *solve, uint32_t blocks) {
-    if (threadIdx.x != 0) return;
+template <bool kB>
+__global__ void k_stats_final(Geo g, SimBufs b, uint32_t chunks) {
+    const uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (bi >= g.nboxes) return;
     const bool is_max[11] = {true, false, true, false, true, false, true, false, true, false, true};
+    const float *part = b.stats_part + (size_t)bi * chunks * 12;
     float out[11];
-    for (int q = 0; q < 11; ++q) out[q] = b.stats_part[q];
-    for (uint32_t k = 1; k < blocks; ++k)
+    for (int q = 0; q < 11; ++q) out[q] = part[q];
+    for (uint32_t k = 1; k < chunks; ++k)
         for (int q = 0; q < 11; ++q) {
-            const float v = b.stats_part[k * 12 + q];
+            const float v = part[k * 12 + q];
             out[q] = is_max[q] ? fmaxf(out[q], v) : fminf(out[q], v);
         }
-    float *s = b.stats;
-    s[0] = (float)((double)*b.stats_acc / kFixedScale / (double)P.count);
-    *b.stats_acc = 0ull;
+    float *s = b.stats + (size_t)bi * 16;
+    s[0] = (float)((double)b.stats_acc[bi] / kFixedScale / (double)params_of<kB>(g, bi).count);
+    b.stats_acc[bi] = 0ull;
     s[1] = fmaxf(out[0], 0.0f);
     s[2] = out[1];
     s[3] = out[2];
@@ -776,8 +841,8 @@ __global__ void k_stats_final(DevParams P, SimBufs b, DevSolve *solve, uint32_t 
     s[5] = out[8];
     s[7] = out[9];
     s[8] = out[10];
-    s[9] = (float)solve->clamp_count;
-    s[10] = (float)solve->nbr_over;
+    s[9] = (float)g.solve[bi].clamp_count;
+    s[10] = (float)g.solve[bi].nbr_over;
 }
 
 // ---- tracers (sim_tracers.wgsl) ----------------------------------------------
@@ -905,47 +970,64 @@ inline uint32_t blocks_for(uint32_t n, uint32_t t) { return (n + t - 1) / t; }
 }  // namespace
 
 void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n) {
-    k_gather<<<blocks_for(n, 256), 256, 0, s>>>(b, n);
+    if (n) k_gather<<<blocks_for(n, 256), 256, 0, s>>>(b, n);
 }
-void launch_density_div(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
-                        DevSolve *solve, unsigned long long *acc) {
-    k_density_div<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, solve, acc);
+
+// One launch of `kern` over g.n particles: the batch instance when the
+// geometry has a box map, the one-box instance otherwise.
+#define FCU_SWEEP(kern, threads, ...)                                                   \
+    do {                                                                                \
+        const uint32_t blocks_ = blocks_for(g.n, threads);                              \
+        if (!blocks_) return;                                                           \
+        if (g.box_of) kern<true><<<blocks_, threads, 0, s>>>(__VA_ARGS__);              \
+        else kern<false><<<blocks_, threads, 0, s>>>(__VA_ARGS__);                      \
+    } while (0)
+
+void launch_density_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot) {
+    FCU_SWEEP(k_density_div, kSolveThreads, g, b, slot);
 }
-void launch_div_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
-                      unsigned long long *acc) {
-    k_div_kappa<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, acc);
+void launch_div_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
+    FCU_SWEEP(k_div_kappa, kSolveThreads, g, b, slot, gate);
 }
-void launch_apply(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
-                  bool add_pressure) {
-    k_apply<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, add_pressure ? 1 : 0);
+void launch_apply(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int gate) {
+    FCU_SWEEP(k_apply, kSolveThreads, g, b, add_pressure ? 1 : 0, gate);
 }
-void launch_forces_eval(cudaStream_t s, const DevParams &P, const SimBufs &b) {
-    k_forces_eval<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b);
+void launch_forces_eval(cudaStream_t s, const Geo &g, const SimBufs &b) {
+    FCU_SWEEP(k_forces_eval, kSolveThreads, g, b);
 }
-void launch_forces_apply(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st) {
-    k_forces_apply<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st);
+void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b) {
+    FCU_SWEEP(k_forces_apply, kSolveThreads, g, b);
 }
-void launch_den_kappa(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
-                      unsigned long long *acc) {
-    k_den_kappa<<<blocks_for(P.count, kSolveThreads), kSolveThreads, 0, s>>>(P, b, st, acc);
+void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
+    FCU_SWEEP(k_den_kappa, kSolveThreads, g, b, slot, gate);
 }
-void launch_integrate(cudaStream_t s, const DevParams &P, const SimBufs &b, const DevStep *st,
-                      DevSolve *solve, int div_slot, int den_slot, int div_iters, int den_iters) {
-    k_integrate<<<blocks_for(P.count, 256), 256, 0, s>>>(P, b, st, solve, div_slot, den_slot,
-                                                         div_iters, den_iters);
+void launch_integrate(cudaStream_t s, const Geo &g, const SimBufs &b, int div_slot, int den_slot,
+                      int div_iters, int den_iters) {
+    FCU_SWEEP(k_integrate, 256, g, b, div_slot, den_slot, div_iters, den_iters);
 }
-void launch_tol_finish(cudaStream_t s, DevSolve *solve, uint32_t n, int which, int first, float tol,
+#undef FCU_SWEEP
+
+void launch_tol_finish(cudaStream_t s, const Geo &g, int which, int first, float tol,
                        uint32_t max_iters, cudaGraphConditionalHandle handle) {
-    k_tol_finish<<<1, 1, 0, s>>>(solve, n, which, first, tol, max_iters, handle);
+    uint32_t threads = (g.nboxes + 31u) & ~31u;
+    if (threads > 256u) threads = 256u;
+    if (threads < 32u) threads = 32u;
+    k_tol_finish<<<1, threads, 0, s>>>(g, which, first, tol, max_iters, handle);
 }
-void launch_stats(cudaStream_t s, const DevParams &P, const SimBufs &b, DevSolve *solve) {
-    uint32_t blocks = blocks_for(P.count, kStatsThreads);
-    if (blocks > kStatsBlocks) blocks = kStatsBlocks;
-    k_stats_partial<<<blocks, kStatsThreads, 0, s>>>(P, b);
-    k_stats_final<<<1, 32, 0, s>>>(P, b, solve, blocks);
+void launch_stats(cudaStream_t s, const Geo &g, const SimBufs &b, uint32_t chunks) {
+    if (!g.nboxes || !chunks) return;
+    const dim3 grid(chunks, g.nboxes);
+    const uint32_t fb = blocks_for(g.nboxes, 128);
+    if (g.box_of) {
+        k_stats_partial<true><<<grid, kStatsThreads, 0, s>>>(g, b);
+        k_stats_final<true><<<fb, 128, 0, s>>>(g, b, chunks);
+    } else {
+        k_stats_partial<false><<<grid, kStatsThreads, 0, s>>>(g, b);
+        k_stats_final<false><<<fb, 128, 0, s>>>(g, b, chunks);
+    }
 }
 void launch_splat(cudaStream_t s, const DevParams &P, const SimBufs &b) {
-    k_splat<<<blocks_for(P.count, 256), 256, 0, s>>>(P, b);
+    if (P.count) k_splat<<<blocks_for(P.count, 256), 256, 0, s>>>(P, b);
 }
 void launch_resolve(cudaStream_t s, const DevParams &P, const SimBufs &b) {
     const uint32_t cells = P.dims[0] * P.dims[1] * P.dims[2];
