@@ -1,0 +1,122 @@
+// grid_static.cu — fluid_grid_build_static: the neighbour-grid build on a
+// scratch area compiled into the library, for callers that cannot allocate.
+//
+// fluid_grid_build needs a device workspace of fluid_grid_workspace_bytes
+// from its caller. Some callers have none to give and may not let the
+// library allocate one: an embedder that owns a fixed GPU memory budget and
+// forbids its libraries to allocate outside it (an engine or visualiser
+// whose pools are sized at start-up), a real-time frame callback in which a
+// cudaMalloc / cudaFree pair would synchronise the device and stall the
+// frame, or a foreign-function caller holding only host handles and no
+// device buffer to pass. This entry point serves them: it allocates nothing
+// (no cudaMalloc, no cudaFree, no allocating library routine) and takes its
+// scratch from one file-scope device array of kStaticScratchBytes.
+//
+// The reference has no counterpart: its grid build always runs on buffers
+// the simulation created with it (crates/fluid-core/src/render.rs:1468-1612).
+//
+// Set-up: the first call on each device, with that device current, looks up
+// the array's device address with cudaGetSymbolAddress (which can load the
+// library's device code); make that first call before any stream capture
+// begins. Later calls on the device reuse the address.
+//
+// Zeroing: every call clears, on the caller's stream and before its kernels,
+// what must start at zero: the cell counts, the look-back status words of
+// the scans and the error word. Everything else in the scratch is written
+// before it is read.
+//
+// Races: there is ONE scratch area per device. Two calls whose work overlaps
+// on the device (different streams, or different host threads, with no
+// stream order or event between them) share it and corrupt each other's
+// result. Order such calls on one stream or with events.
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "grid.cuh"
+
+namespace fcu {
+
+int32_t report_error(int32_t code, const std::string &msg);
+
+namespace {
+
+// 16 MiB: e.g. 2^19 positions over 2^20 cells need 12.1 MiB of scratch,
+// 2^20 positions over 2^18 cells 17.3 MiB (refused).
+constexpr size_t kStaticScratchBytes = (size_t)FLUID_GRID_STATIC_SCRATCH_BYTES;
+static __device__ __align__(256) unsigned char g_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void *g_scratch_addr[kMaxDevices];  // the array's device address, per device
+
+// The scratch address on the current device, looked up on first use.
+cudaError_t scratch_address(int dev, void **out) {
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[dev]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess) return e;
+        g_scratch_addr[dev] = p;
+    }
+    *out = g_scratch_addr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace fcu
+
+using namespace fcu;
+
+extern "C" int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const FluidGrid *grid,
+                                           uint32_t *keys, uint32_t *starts, uint32_t *perm,
+                                           void *stream) {
+    if (!grid || !starts || (n && (!pos4 || !perm)))
+        return report_error(FLUID_ERR_ARG, "fluid_grid_build_static: null argument");
+    if (!(grid->cell > 0.0f)) return report_error(FLUID_ERR_ARG, "fluid_grid_build_static: cell must be positive");
+    for (int i = 0; i < 3; ++i)
+        if (grid->dims[i] == 0) return report_error(FLUID_ERR_ARG, "fluid_grid_build_static: dims must be positive");
+    const uint64_t cells = (uint64_t)grid->dims[0] * grid->dims[1] * grid->dims[2];
+    if (cells >= 0xffffffffull)
+        return report_error(FLUID_ERR_ARG, "fluid_grid_build_static: grid has too many cells");
+    const size_t need = grid_work_bytes(n, (uint32_t)cells);
+    if (need > kStaticScratchBytes) {
+        char msg[256];
+        snprintf(msg, sizeof msg,
+                 "fluid_grid_build_static: %u positions over %llu cells need %zu bytes of scratch, "
+                 "above the fixed %zu; use fluid_grid_build with a workspace",
+                 n, (unsigned long long)cells, need, kStaticScratchBytes);
+        return report_error(FLUID_ERR_ARG, msg);
+    }
+    if ((uintptr_t)pos4 & 15u)
+        return report_error(FLUID_ERR_ARG, "fluid_grid_build_static: positions must be 16-byte aligned");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static: cudaGetDevice: ") +
+                                                cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices)
+        return report_error(FLUID_ERR_ARG, "fluid_grid_build_static: device ordinal above 63");
+    void *ws = nullptr;
+    e = scratch_address(dev, &ws);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static: cudaGetSymbolAddress: ") +
+                                                cudaGetErrorString(e));
+    cudaStream_t st = (cudaStream_t)stream;
+    GridWork w = grid_work_carve(ws, n, (uint32_t)cells, nullptr);
+    e = cudaMemsetAsync(w.err, 0, 4, st);
+    // Without a caller buffer the keys live in k2: pass 0 reads them and
+    // writes k1, and k2 is next written by pass 1, after they are consumed.
+    GridGeom g;
+    for (int i = 0; i < 3; ++i) {
+        g.min[i] = grid->min[i];
+        g.dims[i] = grid->dims[i];
+    }
+    g.cell = grid->cell;
+    if (e == cudaSuccess)
+        e = grid_build_enqueue(st, (const float4 *)pos4, n, g, keys ? keys : w.k2, starts, perm, w, false,
+                               nullptr, nullptr, nullptr, 1);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static: ") + cudaGetErrorString(e));
+    return FLUID_OK;
+}

@@ -146,6 +146,7 @@ def lib():
         "fluid_grid_workspace_bytes": (u64, [u32, C.POINTER(FluidGrid)]),
         "fluid_grid_build": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp, u64, vp]),
         "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
+        "fluid_grid_build_static": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp]),
         "fluid_substep_floor": (u32, [f, f]),
         "fluid_refine_passes": (u32, [f]),
         "fluid_substeps_for": (u32, [f, f, f, u32]),

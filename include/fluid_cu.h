@@ -334,6 +334,23 @@ int32_t fluid_grid_build(const float *pos4, uint32_t n, const FluidGrid *grid, u
 int32_t fluid_grid_build_host(const float *pos4, uint32_t n, const FluidGrid *grid,
                               uint32_t *starts, uint32_t *perm);
 
+/* Scratch bytes compiled into the library for fluid_grid_build_static,
+ * one area per device. */
+#define FLUID_GRID_STATIC_SCRATCH_BYTES (16u << 20)
+
+/* fluid_grid_build for callers that cannot allocate: the same keys, starts
+ * and permutation, with no workspace argument and no allocation of any kind;
+ * the scratch is a fixed area of FLUID_GRID_STATIC_SCRATCH_BYTES inside the
+ * library. No counterpart in the reference (its grid build runs on buffers
+ * the simulation owns). A build needing more scratch than that
+ * (fluid_grid_workspace_bytes above the limit) returns FLUID_ERR_ARG. The
+ * first call on each device sets up the scratch address; make it before any
+ * stream capture begins. One scratch area per device: calls whose work
+ * overlaps on the device race and must be ordered by the caller (one stream,
+ * or events). Asynchronous on `stream`. */
+int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const FluidGrid *grid,
+                                uint32_t *keys, uint32_t *starts, uint32_t *perm, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
