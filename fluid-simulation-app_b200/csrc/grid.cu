@@ -71,6 +71,43 @@ __global__ void __launch_bounds__(256) k_cell_keys(const float4 *__restrict__ po
     }
 }
 
+// The same over a batch of boxes: box b's key is cell_base[b] plus its
+// cell in its own grid. Block 0 moves the substep's nboxes Step blocks
+// (ring entry `cursor`, box-major) into cur[0 .. nboxes-1].
+__global__ void __launch_bounds__(256) k_box_keys(const float4 *__restrict__ pos, uint32_t n,
+                                                  BoxKeys bk, uint32_t *__restrict__ keys,
+                                                  uint32_t *__restrict__ counts,
+                                                  const DevStep *__restrict__ ring, DevStep *cur,
+                                                  DevSolve *solve, uint32_t ring_size) {
+    if (ring && blockIdx.x == 0) {
+        const uint32_t c = solve->cursor;
+        const DevStep *src = ring + (size_t)(c % ring_size) * bk.nboxes;
+        for (uint32_t b = threadIdx.x; b < bk.nboxes; b += blockDim.x) cur[b] = src[b];
+        __syncthreads();
+        if (threadIdx.x == 0) solve->cursor = c + 1u;
+    }
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < n;
+    uint32_t key = 0;
+    if (live) {
+        const uint32_t b = __ldg(&bk.box_of[i]);
+        const DevParams *P = &bk.box[b];
+        const float4 p = __ldg(&pos[i]);
+        const float cell = __ldg(&P->cell);
+        const uint32_t dx = __ldg(&P->dims[0]), dy = __ldg(&P->dims[1]), dz = __ldg(&P->dims[2]);
+        const uint32_t cx = axis_cell(p.x, __ldg(&P->box_min[0]), cell, dx);
+        const uint32_t cy = axis_cell(p.y, __ldg(&P->box_min[1]), cell, dy);
+        const uint32_t cz = axis_cell(p.z, __ldg(&P->box_min[2]), cell, dz);
+        key = __ldg(&bk.cell_base[b]) + (cz * dy + cy) * dx + cx;
+        keys[i] = key;
+    }
+    const uint32_t act = __ballot_sync(0xffffffffu, live);
+    if (live) {
+        const uint32_t peers = __match_any_sync(act, key);
+        if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&counts[key], __popc(peers));
+    }
+}
+
 // Exclusive scan of in[0..n) into out[0..n), single pass. Tiles are claimed
 // in launch order through ctl[0]; ctl[1 + t] is tile t's status word: flag in
 // the high half (1 aggregate, 2 inclusive prefix), value in the low half.
@@ -345,7 +382,7 @@ cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t 
                                const GridGeom &g, uint32_t *keys, uint32_t *starts,
                                uint32_t *perm, GridWork &w, bool counts_zeroed,
                                const DevStep *ring, DevStep *cur, DevSolve *solve,
-                               uint32_t ring_size) {
+                               uint32_t ring_size, const BoxKeys *boxes) {
     cudaError_t e;
     const uint32_t cells = w.cells;
     if (!counts_zeroed) {
@@ -356,7 +393,10 @@ cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t 
     if (e != cudaSuccess) return e;
     if (n > 0 || ring) {
         const uint32_t blocks = div_up(n > 0 ? n : 1, 256);
-        k_cell_keys<<<blocks, 256, 0, stream>>>(pos, n, g, keys, w.counts, ring, cur, solve, ring_size);
+        if (boxes)
+            k_box_keys<<<blocks, 256, 0, stream>>>(pos, n, *boxes, keys, w.counts, ring, cur, solve, ring_size);
+        else
+            k_cell_keys<<<blocks, 256, 0, stream>>>(pos, n, g, keys, w.counts, ring, cur, solve, ring_size);
     }
     unsigned long long *ctl = w.scan_ctl;
     k_scan_lookback<<<div_up(cells > 0 ? cells : 1, kScanTile), kScanThreads, 0, stream>>>(

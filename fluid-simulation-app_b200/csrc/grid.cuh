@@ -52,15 +52,27 @@ size_t grid_work_bytes(uint32_t n, uint32_t cells);
 // Carves `ws` (at least grid_work_bytes) into a GridWork.
 GridWork grid_work_carve(void *ws, uint32_t n, uint32_t cells, uint32_t *err);
 
+// A batch of boxes sharing one grid: slot i belongs to box box_of[i], whose
+// cells are keys cell_base[b] .. cell_base[b] + its cells - 1 (the boxes'
+// cell ranges laid end to end, in box order).
+struct BoxKeys {
+    const uint16_t *box_of;     // [n]
+    const DevParams *box;       // [nboxes]
+    const uint32_t *cell_base;  // [nboxes]
+    uint32_t nboxes;
+};
+
 // Enqueues count -> scan -> stable sort on `stream`. `keys` receives each
 // input's cell key, `starts` the exclusive scan with starts[cells] = n,
 // `perm` the stable permutation. When `counts_zeroed` is false the counts
 // are cleared first. `ring`/`cur`/`solve` (may be null) let the key kernel
-// also fetch the substep's Step block from the ring.
+// also fetch the substep's Step block from the ring. With `boxes`, the keys
+// are the batch's (`g` unused) and every box's Step block of the substep
+// (ring entry cursor holds nboxes of them) moves to cur[0 .. nboxes-1].
 cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t n,
                                const GridGeom &g, uint32_t *keys, uint32_t *starts,
                                uint32_t *perm, GridWork &w, bool counts_zeroed,
                                const DevStep *ring, DevStep *cur, DevSolve *solve,
-                               uint32_t ring_size);
+                               uint32_t ring_size, const BoxKeys *boxes = nullptr);
 
 }  // namespace fcu

@@ -92,6 +92,7 @@ void pack_tracer(const float pos[3], float speed, const float e[2], uint32_t out
 namespace fcu {
 // Records an error for fluid_last_error from another translation unit.
 int32_t report_error(int32_t code, const std::string &msg) { return fail(code, msg); }
+void host_step_constants(float xsph_cfg, const FluidStep &st, DevStep &d);
 }  // namespace fcu
 
 struct FluidSim {
@@ -273,14 +274,7 @@ void seed_tracers(const FluidSimConfig &c, const DevParams &P, uint32_t count,
 }
 
 void fill_step(const FluidSim *s, const FluidStep &st, DevStep &d) {
-    d.s = st;
-    const float dt = st.dt;
-    // The reference evaluates these per thread (sim_solve.wgsl:657, :741;
-    // sim_tracers.wgsl:182); they depend on dt alone, so once per substep.
-    d.xsph_blend = s->cfg.xsph_blend >= 0.0f ? s->cfg.xsph_blend : 1.0f - std::exp(-6.0f * dt);
-    d.chase = 1.0f - std::exp(-20.0f * dt);
-    d.decay = std::exp(-dt / 4.0f);
-    d.pad = 0.0f;
+    host_step_constants(s->cfg.xsph_blend, st, d);
 }
 
 GridGeom geom_of(const DevParams &P) {
@@ -538,6 +532,30 @@ bool valid_config(const FluidSimConfig *c, std::string &why) {
 }
 
 }  // namespace
+
+// Host steps the batch handle (batch.cu) shares with the one-box handle.
+namespace fcu {
+bool host_valid_config(const FluidSimConfig *c, std::string &why) { return valid_config(c, why); }
+void host_params(const FluidSimConfig &c, uint32_t count, DevParams &P) { derive_params(c, count, P); }
+void host_seed(const FluidSimConfig &c, std::vector<float> &pos) {
+    if (c.seeding == FLUID_SEED_SLAB) seed_slab(c.spacing, c.extent, c.fill, pos);
+    else if (c.seeding == FLUID_SEED_BLOCK) seed_block(c, pos);
+    else pos.assign(4ull * c.count, 0.0f);
+}
+// The reference evaluates these per thread (sim_solve.wgsl:657, :741;
+// sim_tracers.wgsl:182); they depend on dt alone, so once per substep.
+void host_step_constants(float xsph_cfg, const FluidStep &st, DevStep &d) {
+    d.s = st;
+    const float dt = st.dt;
+    d.xsph_blend = xsph_cfg >= 0.0f ? xsph_cfg : 1.0f - std::exp(-6.0f * dt);
+    d.chase = 1.0f - std::exp(-20.0f * dt);
+    d.decay = std::exp(-dt / 4.0f);
+    d.pad = 0.0f;
+}
+int32_t host_add_while(cudaStream_t st, cudaGraph_t g, cudaGraphConditionalHandle h, cudaGraph_t *body) {
+    return add_while(st, g, h, body);
+}
+}  // namespace fcu
 
 extern "C" {
 

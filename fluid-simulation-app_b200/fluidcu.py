@@ -147,6 +147,19 @@ def lib():
         "fluid_grid_build": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp, u64, vp]),
         "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
         "fluid_grid_build_static": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp]),
+        "fluid_batch_create": (P, [C.POINTER(FluidSimConfig), u32]),
+        "fluid_batch_destroy": (None, [P]),
+        "fluid_batch_boxes": (u32, [P]),
+        "fluid_batch_count": (u32, [P, u32]),
+        "fluid_batch_total": (u32, [P]),
+        "fluid_batch_stream": (P, [P]),
+        "fluid_batch_params": (i32, [P, u32, C.POINTER(FluidSimParams)]),
+        "fluid_batch_step": (i32, [P, C.POINTER(FluidStep)]),
+        "fluid_batch_run": (i32, [P, C.POINTER(FluidStep), u32]),
+        "fluid_batch_reduce_stats": (i32, [P]),
+        "fluid_batch_stats": (i32, [P, C.POINTER(FluidSimStats)]),
+        "fluid_batch_sync": (i32, [P]),
+        "fluid_batch_get_state": (i32, [P, u32, vp, vp, vp, vp, vp, vp]),
         "fluid_substep_floor": (u32, [f, f]),
         "fluid_refine_passes": (u32, [f]),
         "fluid_substeps_for": (u32, [f, f, f, u32]),
@@ -217,6 +230,69 @@ def make_step(force=(0.0, 0.0, 0.0), dt=0.0, omega=(0.0, 0.0, 0.0), v_clamp=0.0,
     for i, t in enumerate(touches):
         st.touches[i][:] = [float(v) for v in t]
     return st
+
+
+class Batch:
+    """Many independent boxes stepped together: the handle of fluid_batch_create."""
+
+    def __init__(self, cfgs):
+        arr = (FluidSimConfig * len(cfgs))(*cfgs)
+        h = lib().fluid_batch_create(arr, len(cfgs))
+        if not h:
+            raise FluidError(ERR_ARG, "fluid_batch_create: " + lib().fluid_last_error().decode())
+        self.h = h
+        self.nboxes = lib().fluid_batch_boxes(h)
+        self.counts = [lib().fluid_batch_count(h, b) for b in range(self.nboxes)]
+        self.n = lib().fluid_batch_total(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fluid_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def params(self, box):
+        p = FluidSimParams()
+        check(lib().fluid_batch_params(self.h, box, C.byref(p)), "batch_params")
+        return p
+
+    def run(self, steps):
+        """steps: a list of substeps, each a list of nboxes FluidStep."""
+        flat = [s for sub in steps for s in sub]
+        assert len(flat) == len(steps) * self.nboxes
+        arr = (FluidStep * len(flat))(*flat)
+        return check(lib().fluid_batch_run(self.h, arr, len(steps)), "batch_run")
+
+    def step(self, steps):
+        return self.run([steps])
+
+    def reduce_stats(self):
+        return check(lib().fluid_batch_reduce_stats(self.h), "batch_reduce_stats")
+
+    def sync(self):
+        return check(lib().fluid_batch_sync(self.h), "batch_sync")
+
+    def stream(self):
+        return lib().fluid_batch_stream(self.h)
+
+    def stats(self, allow_error=False):
+        arr = (FluidSimStats * self.nboxes)()
+        rc = lib().fluid_batch_stats(self.h, arr)
+        if not allow_error:
+            check(rc, "batch_stats")
+        return list(arr)
+
+    def state(self, box):
+        n = self.counts[box]
+        out = dict(pos=np.zeros((n, 4), np.float32), vel=np.zeros((n, 4), np.float32),
+                   prev_vel=np.zeros((n, 4), np.float32), prev_p=np.zeros(n, np.float32),
+                   temp=np.zeros(n, np.float32), id=np.zeros(n, np.uint32))
+        check(lib().fluid_batch_get_state(self.h, box, *[_p(out[k]) for k in
+                                                         ("pos", "vel", "prev_vel", "prev_p",
+                                                          "temp", "id")]), "batch_get_state")
+        return out
 
 
 class Sim:

@@ -103,6 +103,43 @@ def steps_for(fcu, name, steps, dt=1.0 / 120.0, seed=1, start=0):
             for k, f in enumerate(forces)]
 
 
+BATCH_SPACING = 0.005
+
+
+def batched_boxes(fcu, nboxes=256, seed=3, lo=4096, hi=65536, **kw):
+    """Box configurations of the batched workload: particle counts log-uniform
+    in [lo, hi] (numpy PCG64, `seed`), each box a (2m, m, 2m) lattice block
+    of about that count at 5 mm spacing in a box twice the block on every
+    axis (the tilt_1m shape), its own XSPH coefficient ~ U[0.005, 0.05] and
+    jitter stream."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(math.log(lo), math.log(hi), nboxes))
+    xsph = rng.uniform(0.005, 0.05, nboxes)
+    cfgs = []
+    for b in range(nboxes):
+        m = max(2, int(round((counts[b] / 4.0) ** (1.0 / 3.0))))
+        lat = (2 * m, m, 2 * m)
+        box_hi = tuple(float(F32(2 * x * BATCH_SPACING)) for x in lat)
+        cfgs.append(box_config(fcu, lat, box_hi, BATCH_SPACING, seed=seed * 100003 + b,
+                               xsph=float(F32(xsph[b])), **kw))
+    return cfgs
+
+
+def batched_frame_steps(fcu, nboxes, frames, substeps=4, seed=3, start=0, dt=1.0 / 120.0):
+    """Per-substep Step blocks of the batched workload: box b follows its own
+    tilt sequence (seed * 100003 + b), `substeps` substeps per 1/120 s frame
+    with the frame's body force. Returns [frames * substeps][nboxes]."""
+    dts = float(F32(dt) / F32(substeps))
+    vc = v_clamp(BATCH_SPACING, dts)
+    forces = [tilt_schedule(seed * 100003 + b, start + frames, dt)[start:] for b in range(nboxes)]
+    out = []
+    for k in range(frames):
+        row = [fcu.make_step(force=tuple(float(v) for v in forces[b][k]), dt=dts, v_clamp=vc,
+                             seed=start + k) for b in range(nboxes)]
+        out.extend([row] * substeps)
+    return out
+
+
 def grid_positions(kind, n, side, seed):
     """The 16.7M-position grid workload's three distributions, float4."""
     rng = np.random.default_rng(seed)

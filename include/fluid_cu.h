@@ -308,6 +308,39 @@ int32_t fluid_sim_profile_step(FluidSim *sim, const FluidStep *step, float *ms,
 /* Kernel launches one substep issues at the current schedule (fixed mode). */
 uint32_t fluid_sim_kernels_per_substep(const FluidSim *sim);
 
+/* ---- batched boxes --------------------------------------------------------
+ * Many independent boxes stepped by the same launches: each kernel of a
+ * substep covers every box, a substep is one graph launch, and in the
+ * tolerance mode each box stops its own loops (the graph loops while any box
+ * is above tolerance). Each box's trajectory, iteration counts and residuals
+ * are bit-identical to fluid_sim_create of its configuration. The reference
+ * has no batch (one Sim per renderer, render.rs:1468-1612); this replaces
+ * stepping many Sims one after another. */
+typedef struct FluidBatch FluidBatch;
+
+/* boxes[nboxes] (1..65535): per-box geometry, seeding, xsph_blend and
+ * temperature; solve, div/den_iters, div/den_tol, max_iters, nbr_cap and
+ * device must match boxes[0]; tracers must be 0. Null on failure. */
+FluidBatch *fluid_batch_create(const FluidSimConfig *boxes, uint32_t nboxes);
+void fluid_batch_destroy(FluidBatch *batch);
+uint32_t fluid_batch_boxes(const FluidBatch *batch);
+uint32_t fluid_batch_count(const FluidBatch *batch, uint32_t box);
+uint32_t fluid_batch_total(const FluidBatch *batch);
+void *fluid_batch_stream(FluidBatch *batch);
+int32_t fluid_batch_params(const FluidBatch *batch, uint32_t box, FluidSimParams *out);
+/* One substep of every box; steps[nboxes], box k takes steps[k] (dt > 0). */
+int32_t fluid_batch_step(FluidBatch *batch, const FluidStep *steps);
+/* `count` substeps; steps[count][nboxes]. Asynchronous. */
+int32_t fluid_batch_run(FluidBatch *batch, const FluidStep *steps, uint32_t count);
+/* reduce_stats of every box (sim_solve.wgsl:800-874). */
+int32_t fluid_batch_reduce_stats(FluidBatch *batch);
+/* Per-box statistics, out[nboxes]. Synchronises. */
+int32_t fluid_batch_stats(FluidBatch *batch, FluidSimStats *out);
+int32_t fluid_batch_sync(FluidBatch *batch);
+/* One box's resting set (slot order), as fluid_sim_get_state. */
+int32_t fluid_batch_get_state(FluidBatch *batch, uint32_t box, float *pos4, float *vel4,
+                              float *prev_vel4, float *prev_p, float *temp, uint32_t *id);
+
 /* ---- the neighbour grid alone ------------------------------------------ */
 
 /* Grid geometry: sim.rs:14-44 (Grid). Key of a position:

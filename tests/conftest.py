@@ -35,3 +35,14 @@ def fcu():
     mod = _load_product()
     mod.lib()
     return mod
+
+
+@pytest.fixture(scope="session")
+def wl():
+    import importlib.util
+    path = os.path.join(ROOT, "fluid-simulation-app_b200", "workloads.py")
+    spec = importlib.util.spec_from_file_location("workloads", path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["workloads"] = mod
+    spec.loader.exec_module(mod)
+    return mod
