@@ -15,6 +15,18 @@
 
 namespace fcu {
 
+// Physical constants of the solver (sim_solve.wgsl:84-172, :792).
+constexpr float TOUCH_RATE = 40.0f;
+constexpr float K_NEAR = 3000.0f;
+constexpr float DYNAMIC_VISCOSITY = 1.002e-3f;
+constexpr float HEAT_CAPACITY = 4184.0f;
+constexpr float CONDUCTIVITY = 0.598f;
+constexpr float EXPANSION = 2.07e-4f;
+constexpr float SIGMA_WATER = 0.0728f;
+constexpr float LATTICE_SIGMA = 0.8665f;
+constexpr float COS_CONTACT = -0.342f;
+constexpr float HUGE_F = 1e30f;
+
 // Device error flags (sticky, OR-ed into a device word).
 enum : uint32_t {
     ERRF_SCAN_TIMEOUT = 1u,  // a decoupled look-back wait gave up

@@ -37,18 +37,6 @@ namespace fcu {
 
 namespace {
 
-// sim_solve.wgsl:84-172
-constexpr float TOUCH_RATE = 40.0f;
-constexpr float K_NEAR = 3000.0f;
-constexpr float DYNAMIC_VISCOSITY = 1.002e-3f;
-constexpr float HEAT_CAPACITY = 4184.0f;
-constexpr float CONDUCTIVITY = 0.598f;
-constexpr float EXPANSION = 2.07e-4f;
-constexpr float SIGMA_WATER = 0.0728f;
-constexpr float LATTICE_SIGMA = 0.8665f;
-constexpr float COS_CONTACT = -0.342f;
-constexpr float HUGE_F = 1e30f;  // sim_solve.wgsl:792
-
 __device__ __forceinline__ float kernel_q(const DevParams &P, float q) {  // :176-182
     if (q < 1.0f) return P.sigma * (1.0f - 1.5f * q * q * (1.0f - 0.5f * q));
     const float t = 2.0f - q;

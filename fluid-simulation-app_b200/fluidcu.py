@@ -160,6 +160,15 @@ def lib():
         "fluid_batch_stats": (i32, [P, C.POINTER(FluidSimStats)]),
         "fluid_batch_sync": (i32, [P]),
         "fluid_batch_get_state": (i32, [P, u32, vp, vp, vp, vp, vp, vp]),
+        "fluid_adjoint_create": (P, [C.POINTER(FluidSimConfig), u32, u32, f, f, u32, u32]),
+        "fluid_adjoint_destroy": (None, [P]),
+        "fluid_adjoint_count": (u32, [P]),
+        "fluid_adjoint_forward": (i32, [P, vp, C.c_double, vp, vp]),
+        "fluid_adjoint_backward": (i32, [P, vp, vp]),
+        "fluid_adjoint_get_schedule": (i32, [P, vp, vp]),
+        "fluid_adjoint_set_schedule": (i32, [P, vp, vp]),
+        "fluid_adjoint_final_state": (i32, [P, vp, vp]),
+        "fluid_adjoint_timing": (i32, [P, vp, vp]),
         "fluid_substep_floor": (u32, [f, f]),
         "fluid_refine_passes": (u32, [f]),
         "fluid_substeps_for": (u32, [f, f, f, u32]),
@@ -230,6 +239,65 @@ def make_step(force=(0.0, 0.0, 0.0), dt=0.0, omega=(0.0, 0.0, 0.0), v_clamp=0.0,
     for i, t in enumerate(touches):
         st.touches[i][:] = [float(v) for v in t]
     return st
+
+
+class Adjoint:
+    """The differentiable model and its adjoint: the handle of fluid_adjoint_create."""
+
+    def __init__(self, cfg, frames, substeps_per_frame, frame_dt, v_clamp, checkpoint_every=10,
+                 precision=32):
+        h = lib().fluid_adjoint_create(C.byref(cfg), frames, substeps_per_frame, frame_dt, v_clamp,
+                                       checkpoint_every, precision)
+        if not h:
+            raise FluidError(ERR_ARG, "fluid_adjoint_create: " + lib().fluid_last_error().decode())
+        self.h = h
+        self.frames = frames
+        self.substeps = frames * substeps_per_frame
+        self.n = lib().fluid_adjoint_count(h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().fluid_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def forward(self, forces, xsph, target):
+        f = np.ascontiguousarray(forces, np.float64).reshape(self.frames, 3)
+        t = np.ascontiguousarray(target, np.float64).reshape(3)
+        loss = C.c_double(0.0)
+        check(lib().fluid_adjoint_forward(self.h, _p(f), float(xsph), _p(t), C.byref(loss)),
+              "adjoint_forward")
+        return loss.value
+
+    def backward(self):
+        g = np.zeros((self.frames, 3), np.float64)
+        gx = C.c_double(0.0)
+        check(lib().fluid_adjoint_backward(self.h, _p(g), C.byref(gx)), "adjoint_backward")
+        return g, gx.value
+
+    def schedule(self):
+        d = np.zeros(self.substeps, np.uint32)
+        e = np.zeros(self.substeps, np.uint32)
+        check(lib().fluid_adjoint_get_schedule(self.h, _p(d), _p(e)), "adjoint_get_schedule")
+        return d, e
+
+    def set_schedule(self, div_iters, den_iters):
+        d = np.ascontiguousarray(div_iters, np.uint32)
+        e = np.ascontiguousarray(den_iters, np.uint32)
+        check(lib().fluid_adjoint_set_schedule(self.h, _p(d), _p(e)), "adjoint_set_schedule")
+
+    def final_state(self):
+        p = np.zeros((self.n, 3), np.float64)
+        v = np.zeros((self.n, 3), np.float64)
+        check(lib().fluid_adjoint_final_state(self.h, _p(p), _p(v)), "adjoint_final_state")
+        return p, v
+
+    def timing(self):
+        a, b = C.c_float(0.0), C.c_float(0.0)
+        check(lib().fluid_adjoint_timing(self.h, C.byref(a), C.byref(b)), "adjoint_timing")
+        return a.value, b.value
 
 
 class Batch:

@@ -341,6 +341,43 @@ int32_t fluid_batch_sync(FluidBatch *batch);
 int32_t fluid_batch_get_state(FluidBatch *batch, uint32_t box, float *pos4, float *vel4,
                               float *prev_vel4, float *prev_p, float *temp, uint32_t *id);
 
+/* ---- the adjoint -----------------------------------------------------------
+ * A differentiable model of the substep (density, divergence solve, forces,
+ * density solve, advection; particles in a fixed order, neighbour lists
+ * rebuilt every substep) with hand-written adjoint kernels. Controls: one
+ * body force per frame (the tilt-control sequence) and the XSPH
+ * coefficient. Loss: |COM(final) - target|^2 + mean((rho/rho0 - 1)^2).
+ * Each substep's neighbour lists, iteration counts and clamp branches are
+ * held fixed under differentiation; the counts are decided by the
+ * tolerance rule on the first forward (or set) and then frozen. The state
+ * is checkpointed every `checkpoint_every` frames; the backward pass
+ * recomputes each segment from its checkpoint. Precision 32 or 64 (the
+ * FP64 instance is what finite differences check). The reference has no
+ * adjoint (no counterpart). */
+typedef struct FluidAdjoint FluidAdjoint;
+
+FluidAdjoint *fluid_adjoint_create(const FluidSimConfig *cfg, uint32_t frames,
+                                   uint32_t substeps_per_frame, float frame_dt, float v_clamp,
+                                   uint32_t checkpoint_every, uint32_t precision);
+void fluid_adjoint_destroy(FluidAdjoint *adj);
+uint32_t fluid_adjoint_count(const FluidAdjoint *adj);
+/* forces[frames][3], the XSPH coefficient, target[3]; writes the loss.
+ * Synchronises. */
+int32_t fluid_adjoint_forward(FluidAdjoint *adj, const double *forces, double xsph,
+                              const double target[3], double *loss);
+/* Gradients of the last forward's loss: grad_forces[frames][3], grad_xsph
+ * (either may be null). Needs a forward since the last backward. */
+int32_t fluid_adjoint_backward(FluidAdjoint *adj, double *grad_forces, double *grad_xsph);
+/* The frozen per-substep iteration counts, [frames * substeps_per_frame]. */
+int32_t fluid_adjoint_get_schedule(const FluidAdjoint *adj, uint32_t *div_iters,
+                                   uint32_t *den_iters);
+int32_t fluid_adjoint_set_schedule(FluidAdjoint *adj, const uint32_t *div_iters,
+                                   const uint32_t *den_iters);
+/* Final positions and velocities of the last forward, [count][3]. */
+int32_t fluid_adjoint_final_state(FluidAdjoint *adj, double *pos3, double *vel3);
+/* Device time of the last forward and backward, ms. */
+int32_t fluid_adjoint_timing(const FluidAdjoint *adj, float *forward_ms, float *backward_ms);
+
 /* ---- the neighbour grid alone ------------------------------------------ */
 
 /* Grid geometry: sim.rs:14-44 (Grid). Key of a position:
