@@ -22,6 +22,10 @@ GPU (a single box does not shard), max over ranks.
 batched: the batched-boxes workload (256 boxes, ~5.7M particles) as one
 batch per GPU; with N > 1 the boxes are LPT-sharded across the ranks
 (strong scaling, no collective in the step), device time max over ranks.
+
+adjoint: the adjoint workload (65,536 particles, 120 frames): one forward
+and one backward of the differentiable model, timed on the device, next to
+the production step on the same configuration.
 """
 import argparse
 import ctypes as C
@@ -276,6 +280,7 @@ def cuda_arm(args):
     final = sim.stats()
     sim.close()
     batched = None if args.no_batched else batched_leg(args, fcu, wl, world, rank, local, value / world)
+    adjoint = None if args.no_adjoint else adjoint_leg(args, fcu, wl, world, local)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -309,6 +314,7 @@ def cuda_arm(args):
             "clocks": clocks.summary(),
             "gpu_launches": launches,
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -378,6 +384,65 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
             "compression_avg_mean": float(rows[:, 2].mean()),
             "compression_avg_worst_box": float(rows[:, 2].max()),
             "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu}
+
+
+ADJ_FRAMES = 120
+ADJ_CHECKPOINT = 10
+
+
+def adjoint_leg(args, fcu, wl, world, local):
+    """The adjoint workload: 65,536 particles (64x16x64 block), 120 frames of
+    4 substeps, loss on the final centre of mass and density deviation,
+    gradients with respect to the 120x3 force sequence and the XSPH
+    coefficient, checkpoints every 10 frames. FP32. The first forward
+    decides and freezes the iteration counts (not timed); then one forward
+    and one backward are timed on the device. The production step on the
+    same configuration, 480 substeps in tolerance mode, is timed beside it."""
+    import torch
+    cfg = wl.make_config(fcu, "adjoint_64k", device=local)
+    dt = float(np.float32(1.0 / 120.0))
+    dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
+    vc = wl.v_clamp(0.005, dts)
+    forces = wl.tilt_schedule(2, ADJ_FRAMES, 1.0 / 120.0).astype(np.float64)
+    target = np.array([0.64, 0.05, 0.64])
+    adj = fcu.Adjoint(cfg, ADJ_FRAMES, SUBSTEPS_PER_FRAME, dt, vc, ADJ_CHECKPOINT, precision=32)
+    adj.forward(forces, 0.01, target)
+    div_it, den_it = adj.schedule()
+    loss = adj.forward(forces, 0.01, target)
+    fwd_ms, _ = adj.timing()
+    g, gx = adj.backward()
+    _, bwd_ms = adj.timing()
+    n = adj.n
+    adj.close()
+    # the production step on the same box, same substeps
+    sim = fcu.Sim(cfg)
+    steps = [fcu.make_step(force=tuple(float(v) for v in forces[k // SUBSTEPS_PER_FRAME]), dt=dts,
+                           v_clamp=vc, seed=k) for k in range(ADJ_FRAMES * SUBSTEPS_PER_FRAME)]
+    sim.run(steps[:40])
+    sim.sync()
+    stream = torch.cuda.ExternalStream(sim.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.run(steps)
+    e1.record(stream)
+    e1.synchronize()
+    prod_ms = e0.elapsed_time(e1)
+    sim.close()
+    sub = ADJ_FRAMES * SUBSTEPS_PER_FRAME
+    gv = np.concatenate([g.ravel(), [gx]])
+    return {"workload": "adjoint_64k", "particles": n, "frames": ADJ_FRAMES, "substeps": sub,
+            "checkpoint_every_frames": ADJ_CHECKPOINT, "precision": "f32", "loss": loss,
+            "forward_ms": fwd_ms, "backward_ms": bwd_ms,
+            "value": n * sub / ((fwd_ms + bwd_ms) / 1000.0), "unit": UNIT,
+            "backward_over_model_forward": bwd_ms / fwd_ms,
+            "production_forward_ms": prod_ms,
+            "backward_over_production_forward": bwd_ms / prod_ms,
+            "mean_div_iters": float(div_it.mean()), "mean_den_iters": float(den_it.mean()),
+            "grad_norm": float(np.linalg.norm(gv)) if np.all(np.isfinite(gv)) else None,
+            "grad_note": "sensitivities grow exponentially with the horizon on this splashing "
+                         "workload; the gradient is checked against FP64 central differences "
+                         "on short horizons (tests/test_gpu_adjoint.py)"}
 
 
 def profile_only(args, fcu, wl, sim, forces, dt_sub, w):
@@ -492,6 +557,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-boxes leg")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     ap.add_argument("--profile-substeps", type=int, default=0,
                     help="after the warm-up, run this many substeps as direct launches timed per kernel, then exit")
     args = ap.parse_args()
