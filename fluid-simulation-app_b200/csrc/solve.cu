@@ -27,7 +27,7 @@
 #define FCU_B_PV 4
 #endif
 #ifndef FCU_B_N5
-#define FCU_B_N5 2
+#define FCU_B_N5 1
 #endif
 #ifndef FCU_MINB
 #define FCU_MINB 0
@@ -205,14 +205,51 @@ __device__ __forceinline__ F3 pair_grad(float scale, F3 pos, float4 pj) {
 // batch loads the particle's own record in its empty places and skips them.
 // `use(scale, record)` sees the neighbours in the same order as a plain
 // loop, so every sum is the same sum.
+// A list entry is read once per sweep: with FCU_LIST_CS it is loaded with
+// the streaming (evict-first) hint, leaving the caches to the neighbours'
+// records. With FCU_PREFETCH the entries of the next batch are requested
+// before the current batch's records are used.
+#ifndef FCU_LIST_CS
+#define FCU_LIST_CS 1
+#endif
+#ifndef FCU_PREFETCH
+#define FCU_PREFETCH 1
+#endif
+__device__ __forceinline__ uint2 list_ld(const uint2 *p) {
+#if FCU_LIST_CS
+    return __ldcs(p);
+#else
+    return __ldg(p);
+#endif
+}
+
 template <int B, class T, class Load, class Use>
 __device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, uint32_t i,
                                      uint32_t cnt, Load load, Use use) {
+#if FCU_PREFETCH
+    uint2 e[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u) e[u] = ((uint32_t)u < cnt) ? list_ld(&nbr[(size_t)u * n + i]) : make_uint2(i, 0u);
+    for (uint32_t k = 0; k < cnt; k += B) {
+        T v[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) v[u] = load(e[u].x);
+        uint2 en[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            en[u] = (k + B + u < cnt) ? list_ld(&nbr[(size_t)(k + B + u) * n + i]) : make_uint2(i, 0u);
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (k + u < cnt) use(__uint_as_float(e[u].y), v[u]);
+#pragma unroll
+        for (int u = 0; u < B; ++u) e[u] = en[u];
+    }
+#else
     for (uint32_t k = 0; k < cnt; k += B) {
         uint2 e[B];
 #pragma unroll
         for (int u = 0; u < B; ++u)
-            e[u] = (k + u < cnt) ? __ldg(&nbr[(size_t)(k + u) * n + i]) : make_uint2(i, 0u);
+            e[u] = (k + u < cnt) ? list_ld(&nbr[(size_t)(k + u) * n + i]) : make_uint2(i, 0u);
         T v[B];
 #pragma unroll
         for (int u = 0; u < B; ++u) v[u] = load(e[u].x);
@@ -220,6 +257,7 @@ __device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, 
         for (int u = 0; u < B; ++u)
             if (k + u < cnt) use(__uint_as_float(e[u].y), v[u]);
     }
+#endif
 }
 
 struct PosKd {
@@ -347,16 +385,52 @@ __device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d
 }
 
 // ---- density_div (sim_solve.wgsl:411-518) --------------------------------
-// One thread per particle over its stencil. A warp-uniform two-phase variant
-// (lanes of one cell row walking the union of their ranges, hits staged in
-// shared memory) was measured slower on the 1M-particle workload (1.39
-// against 1.29 ms: ~22 instructions per union candidate at 34 % occupancy),
-// so the plain scan stays. Every candidate of the stencil is taken in order;
-// each hit is summed and the first `cap` are listed.
+// One thread per particle, in rounds of two phases. Phase 1: the thread walks
+// its own stencil candidates in order and stages each hit as a (row, offset)
+// code in its column of shared memory, until kStage hits are staged or the
+// stencil is done. Phase 2: it forms the sums over the staged hits, in order,
+// and writes their list entries. A plain loop that sums each hit where it is
+// found runs the long hit path at every candidate where any lane of the warp
+// hits (ncu: 12 of 32 lanes active per instruction, 73 % issue-bound on the
+// 1M-particle workload) and scatters its list stores; here the warp's lanes
+// take their k-th staged hit together, so the hit path is not divergent and
+// the stores of a round coalesce. The neighbours are summed in the same
+// order as the plain loop, so every sum is the same sum. A stencil row wider
+// than a code's 4,096-slot offset falls back to the plain loop.
+constexpr int kStage = 32;
+constexpr uint32_t kRowSpan = 4096;
+
+// The plain loop over every candidate, each hit summed and the first `cap`
+// listed. Returns the hits found.
+__device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_t base, const SimBufs &b,
+                                                  uint32_t n, uint32_t i, F3 pos, F3 vel,
+                                                  const Stencil &t, DensitySums &d) {
+    uint32_t found = 0;
+    for (int oz = -1; oz <= 1; ++oz)
+        for (int oy = -1; oy <= 1; ++oy) {
+            uint32_t s, e;
+            if (!stencil_row(P, base, b.starts, n, t, oz, oy, s, e)) continue;
+            for (uint32_t k = s; k < e; ++k) {
+                if (k == i) continue;
+                const F3 x = pos - xyz(__ldg(&b.wpos[k]));
+                const float r2 = dot(x, x);
+                if (r2 >= P.support_sq) continue;
+                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
+                if (found < P.nbr_cap) b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
+                found++;
+            }
+        }
+    return found;
+}
+
 template <bool kB>
 __global__ void __launch_bounds__(kSolveThreads) k_density_div(Geo g, SimBufs b, int slot) {
+    __shared__ uint16_t s_hit[kStage][kSolveThreads];
+    __shared__ uint32_t s_beg[9][kSolveThreads];
+    __shared__ uint32_t s_end[9][kSolveThreads];
     const uint32_t n = g.n;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t i = blockIdx.x * blockDim.x + tid;
     const bool live = i < n;
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
@@ -374,21 +448,71 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(Geo g, SimBufs b,
         d.grad_sq = 0.0f;
         d.drho = 0.0f;
         d.grad_sum = f3(0.f, 0.f, 0.f);
+        bool wide = false;
+#pragma unroll
+        for (int r = 0; r < 9; ++r) {
+            uint32_t s = 0, e = 0;
+            if (!stencil_row(P, base, b.starts, n, t, r / 3 - 1, r % 3 - 1, s, e)) s = e = 0;
+            s_beg[r][tid] = s;
+            s_end[r][tid] = e;
+            wide = wide || (e - s > kRowSpan);
+        }
         uint32_t found = 0;
-        for (int oz = -1; oz <= 1; ++oz)
-            for (int oy = -1; oy <= 1; ++oy) {
-                uint32_t s, e;
-                if (!stencil_row(P, base, b.starts, n, t, oz, oy, s, e)) continue;
-                for (uint32_t k = s; k < e; ++k) {
-                    if (k == i) continue;
-                    const F3 x = pos - xyz(__ldg(&b.wpos[k]));
-                    const float r2 = dot(x, x);
-                    if (r2 >= P.support_sq) continue;
-                    const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
-                    if (found < cap) b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
-                    found++;
+        if (!wide) {
+            uint32_t r = 0, k = s_beg[0][tid], e = s_end[0][tid], rs = k;
+            bool more = true;
+            while (more) {
+                // phase 1: stage up to kStage hits
+                uint32_t staged = 0;
+                while (staged < (uint32_t)kStage) {
+                    if (k >= e) {
+                        if (++r >= 9u) {
+                            more = false;
+                            break;
+                        }
+                        k = rs = s_beg[r][tid];
+                        e = s_end[r][tid];
+                        continue;
+                    }
+                    if (k != i) {
+                        const F3 x = pos - xyz(__ldg(&b.wpos[k]));
+                        if (dot(x, x) < P.support_sq) {
+                            s_hit[staged][tid] = (uint16_t)((r << 12) | (k - rs));
+                            ++staged;
+                        }
+                    }
+                    ++k;
                 }
+                // phase 2: the staged hits, in order, two loads in flight
+                for (uint32_t h = 0; h < staged; h += 2) {
+                    uint32_t j[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        const bool ok = h + u < staged;
+                        const uint32_t code = ok ? (uint32_t)s_hit[h + u][tid] : 0u;
+                        j[u] = ok ? s_beg[code >> 12][tid] + (code & (kRowSpan - 1u)) : i;
+                    }
+                    float4 pj[2], vj[2];
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        pj[u] = __ldg(&b.wpos[j[u]]);
+                        vj[u] = __ldg(&b.wvel[j[u]]);
+                    }
+#pragma unroll
+                    for (int u = 0; u < 2; ++u) {
+                        if (h + u < staged) {
+                            const F3 x = pos - xyz(pj[u]);
+                            const float gs = density_pair(P, d, pos, vel, x, dot(x, x), vj[u]);
+                            const uint32_t idx = found + h + u;
+                            if (idx < cap) b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
+                        }
+                    }
+                }
+                found += staged;
             }
+        } else {
+            found = density_scan_all(P, base, b, n, i, pos, vel, t, d);
+        }
         // sim_solve.wgsl:475-517
         b.nbr_n[i] = found < cap ? found : cap;
         if (found > cap) atomicAdd(&g.solve[bi].nbr_over, found - cap);
