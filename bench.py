@@ -55,10 +55,13 @@ SUBSTEPS_PER_FRAME = 4
 ALGO_BYTES = {"grid": 20.0, "gather": 116.0, "density_div": 44.0, "div_kappa": 28.0,
               "div_apply": 36.0, "forces_eval": 84.0, "forces_den_apply": 92.0,
               "den_kappa": 36.0, "den_apply": 36.0, "integrate": 120.0}
-# DRAM bytes per particle per launch, from one ncu capture of each kernel on
-# a 131,072-particle case of the same workload (profiles/; traffic grows in
-# proportion to the particles). None until captured.
-NCU_TRAFFIC_PER_PARTICLE = {}
+# DRAM bytes (read + write) per particle per launch, from ncu captures of
+# each kernel on this workload at its full 1,048,576 particles
+# (profiles/list_sweeps_tilt_1m.md, profiles/density_div_tilt_1m.md).
+NCU_TRAFFIC_PER_PARTICLE = {"den_kappa": (583.2e6 + 5.2e6) / 1048576,
+                            "den_apply": (587.4e6 + 6.7e6) / 1048576,
+                            "div_apply": (587.4e6 + 6.7e6) / 1048576,
+                            "density_div": (66.9e6 + 484.9e6) / 1048576}
 
 
 def load(name, path):
