@@ -326,6 +326,7 @@ int32_t batch_create_into(FluidBatch *s, const FluidSimConfig *boxes, uint32_t n
     BK(s->alloc(&b.density, n));
     BK(s->alloc(&b.alpha, n));
     BK(s->alloc(&b.kd, n));
+    BK(s->alloc(&b.wpk, n));
     BK(s->alloc(&b.pressure, n));
     BK(s->alloc(&b.pinc, n));
     BK(s->alloc(&b.rho_near, n));

@@ -643,6 +643,7 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(s->alloc(&b.density, n));
     CK(s->alloc(&b.alpha, n));
     CK(s->alloc(&b.kd, n));
+    CK(s->alloc(&b.wpk, n));
     CK(s->alloc(&b.pressure, n));
     CK(s->alloc(&b.pinc, n));
     CK(s->alloc(&b.rho_near, n));

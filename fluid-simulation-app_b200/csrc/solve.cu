@@ -538,7 +538,9 @@ __global__ void __launch_bounds__(kSolveThreads) k_density_div(Geo g, SimBufs b,
         const float a = rho / fmaxf(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
         b.alpha[i] = a;
         drho += dot(vel, wg);
-        b.kd[i] = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
+        const float kdv = fmaxf(drho, 0.0f) * a / fmaxf(dt, 1e-9f) / rho;
+        b.kd[i] = kdv;
+        b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
         term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
     }
     add_term<kB>(&g.solve[bi].acc_div[slot], term);
@@ -577,7 +579,9 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(Geo g, Si
         drho = P.mass * drho;
         drho += dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho = __ldg(&b.density[i]);
-        b.kd[i] = fmaxf(drho, 0.0f) * __ldg(&b.alpha[i]) / fmaxf(dt, 1e-9f) / rho;
+        const float kdv = fmaxf(drho, 0.0f) * __ldg(&b.alpha[i]) / fmaxf(dt, 1e-9f) / rho;
+        b.kd[i] = kdv;
+        b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
         term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
     }
     add_term<kB>(&g.solve[bi].acc_div[slot], term);
@@ -588,7 +592,10 @@ __device__ __forceinline__ F3 kappa_sum(const SimBufs &b, uint32_t i, uint32_t n
     const uint32_t cnt = __ldg(&b.nbr_n[i]);
     F3 dv = f3(0.f, 0.f, 0.f);
     walk<FCU_B_KD, PosKd>(
-        b.nbr, n, i, cnt, [&](uint32_t j) { return PosKd{__ldg(&b.wpos[j]), __ldg(&b.kd[j])}; },
+        b.nbr, n, i, cnt, [&](uint32_t j) {
+            const float4 q = __ldg(&b.wpk[j]);
+            return PosKd{q, q.w};
+        },
         [&](float gs, const PosKd &q) { dv = dv + (kd_i + q.kd) * pair_grad(gs, pos, q.p); });
     return dv;
 }
@@ -672,7 +679,9 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_eval(Geo g, 
     b.accel[i] = make_float4(acc.x, acc.y, acc.z, heat);
     b.xsph[i] = make_float4(blend.x, blend.y, blend.z, 0.0f);
     const float half = 0.5f * __ldg(&b.wpp[i]);
-    b.kd[i] = half / (rho_i * rho_i);
+    const float kdv = half / (rho_i * rho_i);
+    b.kd[i] = kdv;
+    b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
     b.pressure[i] = half;
 }
 
@@ -750,7 +759,9 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(Geo g, Si
         drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;
         const float kk = fmaxf(rho_star - rho0, 0.0f) * __ldg(&b.alpha[i]) / (dt * dt);
-        b.kd[i] = kk / rho;
+        const float kdv = kk / rho;
+        b.kd[i] = kdv;
+        b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
         b.pinc[i] = kk * rho;
         term = fixed_term((double)rho_star / (double)rho0 - 1.0);
     }

@@ -22,6 +22,7 @@ struct SimBufs {
     uint32_t *keys, *starts, *perm;
     float *density, *alpha, *kd, *pressure, *pinc, *rho_near;
     float4 *accel, *xsph, *wgrad;
+    float4 *wpk;  // position and kd of the last prediction: apply's one record per neighbour
     // Neighbour list, slot-major (entry k of particle i at k * n + i): the
     // neighbour's slot and the bits of its kernel-gradient scale dw / r,
     // so a sweep forms the gradient (dw / r) * (x_i - x_j) without the
