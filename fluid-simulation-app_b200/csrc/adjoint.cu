@@ -368,7 +368,9 @@ __global__ void __launch_bounds__(256) k_m_pos4(const V3<T> *__restrict__ x, flo
 }
 
 // Neighbour list of every particle (stencil order, grid order inside a
-// cell), density, near density, alpha and the wall gradient.
+// cell), density, near density, alpha and the wall gradient. With `perm`
+// null the particles are in the grid's cell order (slot k is particle k);
+// otherwise slot k holds particle perm[k].
 template <class T>
 __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
                                                            const float4 *__restrict__ pos4,
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const V3<T> xi = x[i];
-    const float4 pf = pos4[i];
+    const float4 pf = make_float4((float)xi.x, (float)xi.y, (float)xi.z, 0.0f);
     const int bx = (int)axis_cell(pf.x, p.box_min[0], p.cell, p.dims[0]);
     const int by = (int)axis_cell(pf.y, p.box_min[1], p.cell, p.dims[1]);
     const int bz = (int)axis_cell(pf.z, p.box_min[2], p.cell, p.dims[2]);
@@ -396,7 +398,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
             uint32_t s = starts[row + cx0], e = starts[row + cx1 + 1];
             if (e > n) e = n;
             for (uint32_t k = s; k < e; ++k) {
-                const uint32_t j = perm[k];
+                const uint32_t j = perm ? perm[k] : k;
                 if (j == i || j >= n) continue;
                 const V3<T> xij = xi - x[j];
                 const T r2 = dot(xij, xij);
@@ -424,6 +426,24 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
     rho[i] = r;
     rhon[i] = near;
     alpha[i] = r / den;
+}
+
+// The substep's state in the grid's cell order: slot k takes particle
+// perm[k] (positions, velocities, previous pressure, id).
+template <class T>
+__global__ void __launch_bounds__(256) k_m_gather(uint32_t n, const uint32_t *__restrict__ perm,
+                                                  const V3<T> *__restrict__ x, const V3<T> *__restrict__ v,
+                                                  const T *__restrict__ pp, const uint32_t *__restrict__ id,
+                                                  V3<T> *xw, V3<T> *vw, T *ppw, uint32_t *idw, uint32_t *perm_out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint32_t j = perm[k];
+    if (j >= n) j = k;  // only after a grid build that gave up
+    xw[k] = x[j];
+    vw[k] = v[j];
+    ppw[k] = pp[j];
+    idw[k] = id[j];
+    perm_out[k] = j;
 }
 
 // d_i = m sum (v_i - v_j).grad W_ij + v_i.wg_i
@@ -988,6 +1008,20 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density(MP<T> p, uint32_t n, 
     atomic_add3(&xbar[i], xs);
 }
 
+// The gather's adjoint: the adjoints of the cell-ordered inputs go back to
+// the order the substep started from (a permutation, so no sums).
+template <class T>
+__global__ void __launch_bounds__(256) k_r_unpermute(uint32_t n, const uint32_t *__restrict__ perm,
+                                                     const V3<T> *__restrict__ xb, const V3<T> *__restrict__ vb,
+                                                     const T *__restrict__ ppb, V3<T> *xo, V3<T> *vo, T *ppo) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t j = perm[k];
+    xo[j] = xb[k];
+    vo[j] = vb[k];
+    ppo[j] = ppb[k];
+}
+
 // The loss's own adjoints: xbar = 2 (com - target) / n, rhobar =
 // 2 (rho / rho0 - 1) / (rho0 n); the rest zero.
 template <class T>
@@ -1035,6 +1069,7 @@ struct Tape {
     std::vector<V3<T> *> vdiv, vden;  // velocities before each apply, and after the loop
     std::vector<T *> kddiv, kdden;
     T *kdf = nullptr;  // warm-start kd
+    uint32_t *perm = nullptr;  // slot k of the substep held particle perm[k] of the state before it
 };
 
 template <class T>
@@ -1057,9 +1092,11 @@ struct AdjImpl : AdjBase {
     // state and its checkpoints
     V3<T> *x = nullptr, *v = nullptr;
     T *pp = nullptr;
+    uint32_t *id = nullptr, *id2 = nullptr;  // particle ids of the state's order
     std::vector<float> x0;
     std::vector<V3<T> *> ck_x, ck_v;
     std::vector<T *> ck_pp;
+    std::vector<uint32_t *> ck_id;
     // forward scratch (one substep) and the backward's segment tapes
     Tape<T> work;
     std::vector<Tape<T>> seg;
@@ -1071,7 +1108,7 @@ struct AdjImpl : AdjBase {
     std::vector<double> forces;
     double xsph = 0.0, target[3] = {0, 0, 0}, com[3] = {0, 0, 0};
     // adjoints
-    V3<T> *xbar = nullptr, *vbar = nullptr, *abar = nullptr, *bbar = nullptr;
+    V3<T> *xbar = nullptr, *vbar = nullptr, *abar = nullptr, *bbar = nullptr, *xbar2 = nullptr, *vbar2 = nullptr;
     T *rhobar = nullptr, *rhonbar = nullptr, *alphabar = nullptr, *kdbar = nullptr, *pbar = nullptr,
       *ppbar = nullptr, *ppbar_next = nullptr;
     double *fbar = nullptr, *cbar = nullptr;
@@ -1099,6 +1136,7 @@ struct AdjImpl : AdjBase {
         if (with_x) {
             AK(alloc(&t.x, N));
             AK(alloc(&t.pp, N));
+            AK(alloc(&t.perm, N));
         }
         AK(alloc(&t.nbr, N * kModelCap));
         AK(alloc(&t.nbr_n, N));
@@ -1155,14 +1193,18 @@ struct AdjImpl : AdjBase {
         AK(alloc(&x, N));
         AK(alloc(&v, N));
         AK(alloc(&pp, N));
+        AK(alloc(&id, N));
+        AK(alloc(&id2, N));
         const uint32_t nck = (frames + ce - 1) / ce + 1;
         ck_x.assign(nck, nullptr);
         ck_v.assign(nck, nullptr);
         ck_pp.assign(nck, nullptr);
+        ck_id.assign(nck, nullptr);
         for (uint32_t k = 0; k < nck; ++k) {
             AK(alloc(&ck_x[k], N));
             AK(alloc(&ck_v[k], N));
             AK(alloc(&ck_pp[k], N));
+            AK(alloc(&ck_id[k], N));
         }
         // the forward's scratch substep holds the longest schedule any substep may take
         int32_t rc = alloc_tape(work, kMaxIters + 1, kMaxIters + 1, true);
@@ -1175,6 +1217,8 @@ struct AdjImpl : AdjBase {
         AK(alloc(&acc, 8));
         AK(alloc(&xbar, N));
         AK(alloc(&vbar, N));
+        AK(alloc(&xbar2, N));
+        AK(alloc(&vbar2, N));
         AK(alloc(&abar, N));
         AK(alloc(&bbar, N));
         AK(alloc(&rhobar, N));
@@ -1191,10 +1235,13 @@ struct AdjImpl : AdjBase {
 
     int32_t load_initial() {
         std::vector<V3<T>> xs(n), zs(n);
+        std::vector<uint32_t> ids(n);
         for (uint32_t i = 0; i < n; ++i) {
             xs[i] = V3<T>{T(x0[4 * i]), T(x0[4 * i + 1]), T(x0[4 * i + 2])};
             zs[i] = V3<T>{T(0), T(0), T(0)};
+            ids[i] = i;
         }
+        AK(cudaMemcpyAsync(id, ids.data(), 4ull * n, cudaMemcpyHostToDevice, stream));
         AK(cudaMemcpyAsync(x, xs.data(), sizeof(V3<T>) * n, cudaMemcpyHostToDevice, stream));
         AK(cudaMemcpyAsync(v, zs.data(), sizeof(V3<T>) * n, cudaMemcpyHostToDevice, stream));
         AK(cudaMemsetAsync(pp, 0, sizeof(T) * n, stream));
@@ -1202,8 +1249,8 @@ struct AdjImpl : AdjBase {
         return FLUID_OK;
     }
 
-    // Neighbour grid of positions xs, then lists and densities into t.
-    int32_t density(const V3<T> *xs, Tape<T> &t) {
+    // Neighbour grid of positions xs (the state's order): starts and perm.
+    int32_t grid(const V3<T> *xs) {
         k_m_pos4<T><<<nblk(n, 256), 256, 0, stream>>>(xs, pos4, n);
         GridGeom g;
         for (int a = 0; a < 3; ++a) {
@@ -1213,6 +1260,14 @@ struct AdjImpl : AdjBase {
         g.cell = P.cell;
         AK(cudaMemsetAsync(gw.err, 0, 4, stream));
         AK(grid_build_enqueue(stream, pos4, n, g, keys, starts, perm, gw, false, nullptr, nullptr, nullptr, 1));
+        return FLUID_OK;
+    }
+
+    // Neighbour grid of positions xs, then lists and densities into t (the
+    // loss's pass over the final state, which is not in its own cell order).
+    int32_t density(const V3<T> *xs, Tape<T> &t) {
+        const int32_t rc = grid(xs);
+        if (rc != FLUID_OK) return rc;
         k_m_density<T><<<nblk(n, kAdjThreads), kAdjThreads, 0, stream>>>(
             mp, n, xs, pos4, starts, perm, t.nbr, t.nbr_n, t.rho, t.rhon, t.alpha, t.wg, over);
         AK(cudaGetLastError());
@@ -1232,12 +1287,14 @@ struct AdjImpl : AdjBase {
     // unless the schedule is frozen, the tolerance rule decides it.
     int32_t substep(uint32_t k, V3<T> f, T c, Tape<T> &t, bool record) {
         const bool decide = !frozen && !record;
-        AK(cudaMemcpyAsync(t.x, x, sizeof(V3<T>) * n, cudaMemcpyDeviceToDevice, stream));
-        AK(cudaMemcpyAsync(t.pp, pp, sizeof(T) * n, cudaMemcpyDeviceToDevice, stream));
-        AK(cudaMemcpyAsync(t.vdiv[0], v, sizeof(V3<T>) * n, cudaMemcpyDeviceToDevice, stream));
-        int32_t rc = density(t.x, t);
+        // the state in cell order, then lists and densities over slots
+        int32_t rc = grid(x);
         if (rc != FLUID_OK) return rc;
+        k_m_gather<T><<<nblk(n, 256), 256, 0, stream>>>(n, perm, x, v, pp, id, t.x, t.vdiv[0], t.pp, id2, t.perm);
+        std::swap(id, id2);
         const uint32_t B = nblk(n, kAdjThreads);
+        k_m_density<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, pos4, starts, nullptr, t.nbr, t.nbr_n, t.rho,
+                                                      t.rhon, t.alpha, t.wg, over);
         // divergence loop
         uint32_t nd = decide ? 0u : div_it[k];
         if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
@@ -1338,6 +1395,7 @@ struct AdjImpl : AdjBase {
                 AK(cudaMemcpyAsync(ck_x[q], x, sizeof(V3<T>) * n, cudaMemcpyDeviceToDevice, stream));
                 AK(cudaMemcpyAsync(ck_v[q], v, sizeof(V3<T>) * n, cudaMemcpyDeviceToDevice, stream));
                 AK(cudaMemcpyAsync(ck_pp[q], pp, sizeof(T) * n, cudaMemcpyDeviceToDevice, stream));
+                AK(cudaMemcpyAsync(ck_id[q], id, 4ull * n, cudaMemcpyDeviceToDevice, stream));
             }
             for (uint32_t s = 0; s < spf; ++s) {
                 const uint32_t k = fr * spf + s;
@@ -1420,7 +1478,10 @@ struct AdjImpl : AdjBase {
         }
         k_r_density<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.nbr, t.nbr_n, t.rho, rhobar, rhonbar, alphabar,
                                                       xbar);
-        std::swap(ppbar, ppbar_next);
+        // back to the order the substep started from
+        k_r_unpermute<T><<<B2, 256, 0, stream>>>(n, t.perm, xbar, vbar, ppbar, xbar2, vbar2, ppbar_next);
+        std::swap(xbar, xbar2);
+        std::swap(vbar, vbar2);
     }
 
     int32_t backward(double *grad_forces, double *grad_xsph) override {
@@ -1450,6 +1511,7 @@ struct AdjImpl : AdjBase {
             AK(cudaMemcpyAsync(x, ck_x[q], sizeof(V3<T>) * n, cudaMemcpyDeviceToDevice, stream));
             AK(cudaMemcpyAsync(v, ck_v[q], sizeof(V3<T>) * n, cudaMemcpyDeviceToDevice, stream));
             AK(cudaMemcpyAsync(pp, ck_pp[q], sizeof(T) * n, cudaMemcpyDeviceToDevice, stream));
+            AK(cudaMemcpyAsync(id, ck_id[q], 4ull * n, cudaMemcpyDeviceToDevice, stream));
             for (uint32_t k = f0 * spf; k < f1 * spf; ++k) {
                 rc = substep(k, force_of(k), T(xsph), seg[k - f0 * spf], true);
                 if (rc != FLUID_OK) return rc;
@@ -1485,19 +1547,22 @@ struct AdjImpl : AdjBase {
         if (!have_forward) return report_error(FLUID_ERR_STATE, "adjoint: no forward state to read");
         AK(cudaSetDevice(device));
         std::vector<V3<T>> a(n), b(n);
+        std::vector<uint32_t> ids(n);
         AK(cudaMemcpyAsync(a.data(), x, sizeof(V3<T>) * n, cudaMemcpyDeviceToHost, stream));
         AK(cudaMemcpyAsync(b.data(), v, sizeof(V3<T>) * n, cudaMemcpyDeviceToHost, stream));
+        AK(cudaMemcpyAsync(ids.data(), id, 4ull * n, cudaMemcpyDeviceToHost, stream));
         AK(cudaStreamSynchronize(stream));
-        for (uint32_t i = 0; i < n; ++i) {
+        for (uint32_t k = 0; k < n; ++k) {
+            const uint32_t i = ids[k] < n ? ids[k] : k;
             if (pos3) {
-                pos3[3 * i] = (double)a[i].x;
-                pos3[3 * i + 1] = (double)a[i].y;
-                pos3[3 * i + 2] = (double)a[i].z;
+                pos3[3 * i] = (double)a[k].x;
+                pos3[3 * i + 1] = (double)a[k].y;
+                pos3[3 * i + 2] = (double)a[k].z;
             }
             if (vel3) {
-                vel3[3 * i] = (double)b[i].x;
-                vel3[3 * i + 1] = (double)b[i].y;
-                vel3[3 * i + 2] = (double)b[i].z;
+                vel3[3 * i] = (double)b[k].x;
+                vel3[3 * i + 1] = (double)b[k].y;
+                vel3[3 * i + 2] = (double)b[k].z;
             }
         }
         return FLUID_OK;
