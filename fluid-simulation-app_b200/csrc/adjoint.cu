@@ -683,7 +683,17 @@ __global__ void __launch_bounds__(256) k_r_integrate(MP<T> p, uint32_t n, T dt, 
     vbar[i] = vcb;
 }
 
-// apply: given vbar (adjoint of v_out), add the adjoints of kd (kdbar) and x.
+// ---- reverse sweeps, gathered ------------------------------------------------
+// The neighbour lists are symmetric: j lists i exactly when i lists j (both
+// test the same squared distance, x_i - x_j and x_j - x_i differ only in
+// sign). So the share that a pair (i, j) adds to particle j's adjoints through
+// particle i's equation can be formed by j itself, from i's stored adjoints.
+// Every reverse sweep below writes only its own particle's entries, with no
+// atomics; the pair terms are evaluated once from each end.
+
+// apply (v_out = v_in - dt (m sum (kd_i + kd_j) grad W_ij + kd_i wg_i)):
+// given vbar (the adjoint of v_out, and of v_in), write the adjoint of kd and
+// add the adjoint of x.
 template <class T>
 __global__ void __launch_bounds__(kAdjThreads) k_r_apply(MP<T> p, uint32_t n, T dt, const V3<T> *__restrict__ x,
                                                          const uint32_t *__restrict__ nbr,
@@ -696,40 +706,38 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_apply(MP<T> p, uint32_t n, T 
     const T kdi = kd[i];
     const T c = -dt * p.m;
     const uint32_t cnt = nbr_n[i];
-    V3<T> gsum = zero3<T>(), xs = zero3<T>();
+    T s = T(0);
+    V3<T> xs = zero3<T>();
     for (uint32_t k = 0; k < cnt; ++k) {
         const uint32_t j = nbr[(size_t)k * n + i];
         const V3<T> xij = xi - x[j];
         const Radial<T> R = radial(p, dot(xij, xij));
-        const V3<T> gw = R.gs * xij;
-        gsum = gsum + gw;
-        atomicAdd(&kdbar[j], c * dot(gw, vb));
-        const V3<T> hv = (c * (kdi + kd[j])) * hess(R, xij, vb);
-        xs = xs + hv;
-        atomic_add3(&xbar[j], -hv);
+        const V3<T> dvb = vb - vbar[j];
+        s += dot(R.gs * xij, dvb);
+        xs = xs + (c * (kdi + kd[j])) * hess(R, xij, dvb);
     }
     const V3<T> wgi = wg[i];
-    atomicAdd(&kdbar[i], -dt * dot(p.m * gsum + wgi, vb));
+    kdbar[i] = -dt * (p.m * s + dot(wgi, vb));
     const J3<T> J = wall_grad_jac(p, xi);
-    atomic_add3(&xbar[i], xs + (-dt * kdi) * jt_mul(J, vb));
+    xbar[i] = xbar[i] + xs + (-dt * kdi) * jt_mul(J, vb);
 }
 
-// kappa (div: kd = max(d,0) a / dt / rho; den: kk = max(rho + dt d - rho0, 0)
-// a / dt^2, kd = kk / rho, pinc = kk rho): given kdbar and pbar (the
-// pressure's adjoint), add the adjoints of v, x, rho and alpha.
+// kappa, first pass (div: kd = max(d,0) a / dt / rho; den: kk = max(rho +
+// dt d - rho0, 0) a / dt^2, kd = kk / rho, pinc = kk rho): from kdbar and
+// pbar (the pressure's adjoint), the adjoint of the divergence d (dbar) and
+// the particle's own shares of the adjoints of rho and alpha.
 template <class T>
-__global__ void __launch_bounds__(kAdjThreads) k_r_kappa(MP<T> p, uint32_t n, int den, T dt,
-                                                         const V3<T> *__restrict__ x, const V3<T> *__restrict__ v,
-                                                         const uint32_t *__restrict__ nbr,
-                                                         const uint32_t *__restrict__ nbr_n, const T *__restrict__ rho,
-                                                         const T *__restrict__ alpha, const V3<T> *__restrict__ wg,
-                                                         const T *__restrict__ kdbar, const T *__restrict__ pbar,
-                                                         V3<T> *vbar, V3<T> *xbar, T *rhobar, T *alphabar) {
+__global__ void __launch_bounds__(kAdjThreads) k_r_kappa_a(MP<T> p, uint32_t n, int den, T dt,
+                                                           const V3<T> *__restrict__ x, const V3<T> *__restrict__ v,
+                                                           const uint32_t *__restrict__ nbr,
+                                                           const uint32_t *__restrict__ nbr_n,
+                                                           const T *__restrict__ rho, const T *__restrict__ alpha,
+                                                           const V3<T> *__restrict__ wg, const T *__restrict__ kdbar,
+                                                           const T *__restrict__ pbar, T *dbar, T *rhobar,
+                                                           T *alphabar) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t cnt = nbr_n[i];
-    const V3<T> wgi = wg[i];
-    const T d = div_of(p, n, i, x, v, nbr, cnt, wgi);
+    const T d = div_of(p, n, i, x, v, nbr, nbr_n[i], wg[i]);
     const T r = rho[i], a = alpha[i], kb = kdbar[i];
     T db = T(0), rb = T(0), ab = T(0);
     if (!den) {
@@ -751,31 +759,47 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_kappa(MP<T> p, uint32_t n, in
             db = eb * dt;
         }
     }
+    dbar[i] = db;
     rhobar[i] += rb;
     alphabar[i] += ab;
-    if (db == T(0)) return;
+}
+
+// kappa, second pass: d_i = m sum (v_i - v_j).grad W_ij + v_i.wg_i, so
+// vbar_i += m sum (dbar_i + dbar_j) grad W_ij + dbar_i wg_i and
+// xbar_i += m sum (dbar_i + dbar_j) H_ij (v_i - v_j) + dbar_i Jwg^T v_i.
+template <class T>
+__global__ void __launch_bounds__(kAdjThreads) k_r_kappa_b(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
+                                                           const V3<T> *__restrict__ v,
+                                                           const uint32_t *__restrict__ nbr,
+                                                           const uint32_t *__restrict__ nbr_n,
+                                                           const V3<T> *__restrict__ wg, const T *__restrict__ dbar,
+                                                           V3<T> *vbar, V3<T> *xbar) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     const V3<T> xi = x[i], vi = v[i];
-    const T c = db * p.m;
-    V3<T> gsum = zero3<T>(), xs = zero3<T>();
+    const T di = dbar[i];
+    const uint32_t cnt = nbr_n[i];
+    V3<T> vs = zero3<T>(), xs = zero3<T>();
     for (uint32_t k = 0; k < cnt; ++k) {
         const uint32_t j = nbr[(size_t)k * n + i];
+        const T c = p.m * (di + dbar[j]);
+        if (c == T(0)) continue;
         const V3<T> xij = xi - x[j];
         const Radial<T> R = radial(p, dot(xij, xij));
-        const V3<T> gw = R.gs * xij;
-        gsum = gsum + gw;
-        atomic_add3(&vbar[j], (-c) * gw);
-        const V3<T> hv = c * hess(R, xij, vi - v[j]);
-        xs = xs + hv;
-        atomic_add3(&xbar[j], -hv);
+        vs = vs + (c * R.gs) * xij;
+        xs = xs + c * hess(R, xij, vi - v[j]);
     }
-    atomic_add3(&vbar[i], c * gsum + db * wgi);
-    const J3<T> J = wall_grad_jac(p, xi);
-    atomic_add3(&xbar[i], xs + db * jt_mul(J, vi));
+    vbar[i] = vbar[i] + vs + di * wg[i];
+    if (di != T(0)) {
+        const J3<T> J = wall_grad_jac(p, xi);
+        xs = xs + di * jt_mul(J, vi);
+    }
+    xbar[i] = xbar[i] + xs;
 }
 
 // forces_apply: given vbar (adjoint of v_out; the same for v_in), store the
-// adjoints of accel (dt vbar) and blend (c vbar), add those of the force, of
-// the XSPH coefficient, of the warm-start kd and of x.
+// adjoints of accel (dt vbar) and blend (c vbar), write the adjoint of the
+// warm-start kd, add those of the force, of the XSPH coefficient and of x.
 template <class T>
 __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_t n, T dt, T c,
                                                                 const V3<T> *__restrict__ x,
@@ -798,22 +822,20 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_
         const T kdi = kd[i];
         const T cc = -dt * p.m;
         const uint32_t cnt = nbr_n[i];
-        V3<T> gsum = zero3<T>(), xs = zero3<T>();
+        T s = T(0);
+        V3<T> xs = zero3<T>();
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t j = nbr[(size_t)k * n + i];
             const V3<T> xij = xi - x[j];
             const Radial<T> R = radial(p, dot(xij, xij));
-            const V3<T> gw = R.gs * xij;
-            gsum = gsum + gw;
-            atomicAdd(&kdbar[j], cc * dot(gw, vb));
-            const V3<T> hv = (cc * (kdi + kd[j])) * hess(R, xij, vb);
-            xs = xs + hv;
-            atomic_add3(&xbar[j], -hv);
+            const V3<T> dvb = vb - vbar[j];
+            s += dot(R.gs * xij, dvb);
+            xs = xs + (cc * (kdi + kd[j])) * hess(R, xij, dvb);
         }
         const V3<T> wgi = wg[i];
-        atomicAdd(&kdbar[i], -dt * dot(p.m * gsum + wgi, vb));
+        kdbar[i] = -dt * (p.m * s + dot(wgi, vb));
         const J3<T> J = wall_grad_jac(p, xi);
-        atomic_add3(&xbar[i], xs + (-dt * kdi) * jt_mul(J, vb));
+        xbar[i] = xbar[i] + xs + (-dt * kdi) * jt_mul(J, vb);
     }
     for (int q = 0; q < 4; ++q) {
         double t = red[q];
@@ -823,9 +845,100 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_
     }
 }
 
+// One pair's share of forces_eval in particle a's equation (neighbour b,
+// x_ab = x_a - x_b, dv = v_a - v_b), reversed: given a's accel and blend
+// adjoints, the adjoints of x_ab, dv, rho_a, rho_b and of (near_a + near_b).
+template <class T>
+struct PairBar {
+    V3<T> gx, gdv;
+    T rb_a, rb_b, nb;
+};
+template <class T>
+DEV PairBar<T> forces_pair_bar(const MP<T> &p, V3<T> xab, T r2, const Radial<T> &R, V3<T> dv, T rho_a, T rho_b,
+                               T near_a, T near_b, V3<T> ab, V3<T> bb) {
+    PairBar<T> o;
+    o.gx = zero3<T>();
+    o.gdv = zero3<T>();
+    o.rb_a = T(0);
+    o.rb_b = T(0);
+    const T r = R.r;
+    const V3<T> ab_near = p.k_near * ab, ab_ten = p.gamma * ab;
+    // viscosity: visc_k m / (rho_a rho_b) phi(r) dv, phi = gs r^2 / (r^2 + eps)
+    {
+        const T den = r2 + p.eps;
+        const T phi = R.gs * r2 / den;
+        const T s = p.visc_k * p.m / (rho_a * rho_b) * phi;
+        o.gdv = o.gdv + s * ab;
+        const T sb = dot(ab, dv);
+        o.rb_a += -sb * s / rho_a;
+        o.rb_b += -sb * s / rho_b;
+        if (r >= T(1e-9f)) {
+            // dphi/dr = (gs' r^2 + 2 gs r) / den - gs r^2 2 r / den^2
+            const T dphi = (R.dgs * r2 + T(2) * R.gs * r) / den - R.gs * r2 * T(2) * r / (den * den);
+            const T phib = sb * p.visc_k * p.m / (rho_a * rho_b);
+            o.gx = o.gx + (phib * dphi / r) * xab;
+        }
+    }
+    // near pressure: (near_a + near_b) psi(r) x, psi = wn^2 / max(r, 1e-5)
+    {
+        const T wn = R.q < T(1) ? T(1) - R.q : T(0);
+        const T rr = r > T(1e-5f) ? r : T(1e-5f);
+        const T psi = wn * wn / rr;
+        const T sn = near_a + near_b;
+        const T xa = dot(xab, ab_near);
+        o.nb = psi * xa;
+        T dpsi = T(0);
+        if (wn > T(0)) {
+            dpsi = T(2) * wn * (-p.inv_h) / rr;
+            if (r > T(1e-5f)) dpsi -= wn * wn / (r * r);
+        }
+        o.gx = o.gx + (sn * psi) * ab_near;
+        if (r >= T(1e-9f)) o.gx = o.gx + (sn * dpsi / r * xa) * xab;
+    }
+    // XSPH blend: -(m / rho_b) W dv
+    {
+        const T s = p.m / rho_b * R.W;
+        o.gdv = o.gdv - s * bb;
+        const T bdv = dot(bb, dv);
+        o.rb_b += s / rho_b * bdv;
+        if (r >= T(1e-9f)) o.gx = o.gx + (-(p.m / rho_b) * bdv * R.dW / r) * xab;
+    }
+    // surface tension: -corr m chi(r) x, chi = C(r) / max(r, 1e-9)
+    {
+        T C = T(0), dC = T(0);
+        if (r < p.coh_c && r >= T(1e-9f)) {
+            const T cr = p.coh_c - r;
+            const T a = cr * cr * cr * r * r * r;
+            const T da = T(-3) * cr * cr * r * r * r + T(3) * cr * cr * cr * r * r;
+            if (T(2) * r > p.coh_c) {
+                C = p.coh_k * a;
+                dC = p.coh_k * da;
+            } else {
+                C = p.coh_k * (T(2) * a - p.coh_near);
+                dC = p.coh_k * T(2) * da;
+            }
+        }
+        const T rt = r > T(1e-9f) ? r : T(1e-9f);
+        const T chi = C / rt;
+        const T dchi = r > T(1e-9f) ? dC / r - C / (r * r) : T(0);
+        const T sr = rho_a + rho_b;
+        const T corr = T(2) * p.rho0 / sr;
+        const T xa = dot(xab, ab_ten);
+        const T corrb = -p.m * chi * xa;
+        const T srb = -corrb * T(2) * p.rho0 / (sr * sr);
+        o.rb_a += srb;
+        o.rb_b += srb;
+        o.gx = o.gx - (corr * p.m * chi) * ab_ten;
+        if (r >= T(1e-9f)) o.gx = o.gx - (corr * p.m * dchi / r * xa) * xab;
+    }
+    return o;
+}
+
 // forces_eval: given abar, bbar (adjoints of accel and blend), kdbar (of the
 // warm-start kd = pp / (2 rho^2)) and pbar (of pressure = pp / 2), add the
-// adjoints of x, v, rho, near density and the previous pressure.
+// adjoints of x, v, rho and near density, and write that of the previous
+// pressure. Each pair is reversed in the particle's own equation and in the
+// neighbour's.
 template <class T>
 __global__ void __launch_bounds__(kAdjThreads) k_r_forces_eval(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
                                                                const V3<T> *__restrict__ v,
@@ -842,7 +955,6 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_eval(MP<T> p, uint32_t
     const V3<T> xi = x[i], vi = v[i];
     const T rho_i = rho[i], near_i = rhon[i];
     const V3<T> ab = abar[i], bb = bbar[i];
-    const V3<T> ab_near = p.k_near * ab, ab_ten = p.gamma * ab;
     // own terms: kd = half / rho^2, pressure = half, half = pp / 2
     const T kb = kdbar[i];
     ppbar[i] = T(0.5f) * kb / (rho_i * rho_i) + T(0.5f) * pbar[i];
@@ -855,107 +967,33 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_eval(MP<T> p, uint32_t
         const V3<T> xij = xi - x[j];
         const T r2 = dot(xij, xij);
         const Radial<T> R = radial(p, r2);
-        const T r = R.r;
-        const T rho_j = rho[j];
+        const T rho_j = rho[j], near_j = rhon[j];
         const V3<T> dv = vi - v[j];
-        V3<T> gx = zero3<T>();  // adjoint of x_ij from this pair
-        V3<T> gdv = zero3<T>();  // adjoint of dv
-        T rb_j = T(0), nb = T(0);
-        // viscosity: visc_k m / (rho_i rho_j) phi(r) dv, phi = gs r^2 / (r^2 + eps)
-        {
-            const T den = r2 + p.eps;
-            const T phi = R.gs * r2 / den;
-            const T s = p.visc_k * p.m / (rho_i * rho_j) * phi;
-            gdv = gdv + s * ab;
-            const T sb = dot(ab, dv);
-            rb_i += -sb * s / rho_i;
-            rb_j += -sb * s / rho_j;
-            if (r >= T(1e-9f)) {
-                // dphi/dr = (gs' r^2 + 2 gs r) / den - gs r^2 2 r / den^2
-                const T dphi = (R.dgs * r2 + T(2) * R.gs * r) / den - R.gs * r2 * T(2) * r / (den * den);
-                const T phib = sb * p.visc_k * p.m / (rho_i * rho_j);
-                gx = gx + (phib * dphi / r) * xij;
-            }
-        }
-        // near pressure: (near_i + near_j) psi(r) x, psi = wn^2 / max(r, 1e-5)
-        {
-            const T wn = R.q < T(1) ? T(1) - R.q : T(0);
-            const T rr = r > T(1e-5f) ? r : T(1e-5f);
-            const T psi = wn * wn / rr;
-            const T sn = near_i + rhon[j];
-            const T xa = dot(xij, ab_near);
-            nb = psi * xa;  // adjoint of (near_i + near_j)
-            T dpsi = T(0);
-            if (wn > T(0)) {
-                dpsi = T(2) * wn * (-p.inv_h) / rr;
-                if (r > T(1e-5f)) dpsi -= wn * wn / (r * r);
-            }
-            gx = gx + (sn * psi) * ab_near;
-            if (r >= T(1e-9f)) gx = gx + (sn * dpsi / r * xa) * xij;
-        }
-        // XSPH blend: -(m / rho_j) W dv
-        {
-            const T s = p.m / rho_j * R.W;
-            gdv = gdv - s * bb;
-            const T bdv = dot(bb, dv);
-            rb_j += s / rho_j * bdv;
-            if (r >= T(1e-9f)) gx = gx + (-(p.m / rho_j) * bdv * R.dW / r) * xij;
-        }
-        // surface tension: -corr m chi(r) x, chi = C(r) / max(r, 1e-9)
-        {
-            T C = T(0), dC = T(0);
-            if (r < p.coh_c && r >= T(1e-9f)) {
-                const T cr = p.coh_c - r;
-                const T a = cr * cr * cr * r * r * r;
-                const T da = T(-3) * cr * cr * r * r * r + T(3) * cr * cr * cr * r * r;
-                if (T(2) * r > p.coh_c) {
-                    C = p.coh_k * a;
-                    dC = p.coh_k * da;
-                } else {
-                    C = p.coh_k * (T(2) * a - p.coh_near);
-                    dC = p.coh_k * T(2) * da;
-                }
-            }
-            const T rt = r > T(1e-9f) ? r : T(1e-9f);
-            const T chi = C / rt;
-            const T dchi = r > T(1e-9f) ? dC / r - C / (r * r) : T(0);
-            const T sr = rho_i + rho_j;
-            const T corr = T(2) * p.rho0 / sr;
-            const T xa = dot(xij, ab_ten);
-            const T corrb = -p.m * chi * xa;
-            const T srb = -corrb * T(2) * p.rho0 / (sr * sr);
-            rb_i += srb;
-            rb_j += srb;
-            gx = gx - (corr * p.m * chi) * ab_ten;
-            if (r >= T(1e-9f)) gx = gx - (corr * p.m * dchi / r * xa) * xij;
-        }
-        xs = xs + gx;
-        atomic_add3(&xbar[j], -gx);
-        vs = vs + gdv;
-        atomic_add3(&vbar[j], -gdv);
-        atomicAdd(&rhobar[j], rb_j);
-        nb_i += nb;
-        atomicAdd(&rhonbar[j], nb);
+        const PairBar<T> own = forces_pair_bar(p, xij, r2, R, dv, rho_i, rho_j, near_i, near_j, ab, bb);
+        const PairBar<T> oth = forces_pair_bar(p, -xij, r2, R, -dv, rho_j, rho_i, near_j, near_i, abar[j], bbar[j]);
+        xs = xs + own.gx - oth.gx;
+        vs = vs + own.gdv - oth.gdv;
+        rb_i += own.rb_a + oth.rb_b;
+        nb_i += own.nb + oth.nb;
     }
     const J3<T> Ja = wall_adh_jac(p, xi);
     xs = xs + (p.beta * p.rho0) * jt_mul(Ja, ab);
-    atomic_add3(&xbar[i], xs);
-    atomic_add3(&vbar[i], vs);
-    atomicAdd(&rhobar[i], rb_i);
-    atomicAdd(&rhonbar[i], nb_i);
+    xbar[i] = xbar[i] + xs;
+    vbar[i] = vbar[i] + vs;
+    rhobar[i] += rb_i;
+    rhonbar[i] += nb_i;
 }
 
-// density: given rhobar, rhonbar, alphabar (complete), add the adjoint of x
-// through rho = m (sigma + sum W) + rho0 fill(x), near = sum wn^3 and
-// alpha = rho / max(|G|^2 + S, 1e-4), G = m sum grad W + wg(x),
-// S = m^2 sum |grad W|^2.
+// density, first pass: with rhobar, alphabar complete, the total adjoint of
+// rho (through rho itself and alpha = rho / max(|G|^2 + S, 1e-4)) and those
+// of G = m sum grad W + wg(x) and S = m^2 sum |grad W|^2.
 template <class T>
-__global__ void __launch_bounds__(kAdjThreads) k_r_density(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
-                                                           const uint32_t *__restrict__ nbr,
-                                                           const uint32_t *__restrict__ nbr_n,
-                                                           const T *__restrict__ rho, const T *__restrict__ rhobar,
-                                                           const T *__restrict__ rhonbar,
-                                                           const T *__restrict__ alphabar, V3<T> *xbar) {
+__global__ void __launch_bounds__(kAdjThreads) k_r_density_a(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
+                                                             const uint32_t *__restrict__ nbr,
+                                                             const uint32_t *__restrict__ nbr_n,
+                                                             const T *__restrict__ rho, const T *__restrict__ rhobar,
+                                                             const T *__restrict__ alphabar, T *rbt, V3<T> *gbar,
+                                                             T *sbar) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const V3<T> xi = x[i];
@@ -970,8 +1008,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density(MP<T> p, uint32_t n, 
         gsum = gsum + gw;
         gsq += dot(gw, gw);
     }
-    const V3<T> wgi = wall_grad(p, xi);
-    const V3<T> G = p.m * gsum + wgi;
+    const V3<T> G = p.m * gsum + wall_grad(p, xi);
     const T den = dot(G, G) + p.m * p.m * gsq;
     const T r = rho[i];
     const T ab = alphabar[i];
@@ -986,26 +1023,53 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density(MP<T> p, uint32_t n, 
     } else {
         rb += ab / T(1e-4f);
     }
-    const T nb = rhonbar[i];
+    rbt[i] = rb;
+    gbar[i] = Gb;
+    sbar[i] = Sb;
+}
+
+// The gradient, with respect to x_ab, of particle a's density-pass terms
+// weighted by its adjoints: rho (rb m grad W), G (m H Gb), S (2 Sb m^2 H
+// grad W) and near density (nb 3 wn^2 d wn / d x).
+template <class T>
+DEV V3<T> density_pair_bar(const MP<T> &p, V3<T> xab, const Radial<T> &R, T rb, V3<T> Gb, T Sb, T nb) {
+    const V3<T> gw = R.gs * xab;
+    V3<T> g = (rb * p.m) * gw;
+    g = g + p.m * hess(R, xab, Gb);
+    g = g + (Sb * p.m * p.m * T(2)) * hess(R, xab, gw);
+    if (R.q < T(1) && R.r >= T(1e-9f)) {
+        const T wn = T(1) - R.q;
+        g = g + (nb * T(3) * wn * wn * (-p.inv_h) / R.r) * xab;
+    }
+    return g;
+}
+
+// density, second pass: add the adjoint of x from every pair, reversed in
+// the particle's own terms and in the neighbour's, and from the walls.
+template <class T>
+__global__ void __launch_bounds__(kAdjThreads) k_r_density_b(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
+                                                             const uint32_t *__restrict__ nbr,
+                                                             const uint32_t *__restrict__ nbr_n,
+                                                             const T *__restrict__ rbt, const V3<T> *__restrict__ gbar,
+                                                             const T *__restrict__ sbar,
+                                                             const T *__restrict__ rhonbar, V3<T> *xbar) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const V3<T> xi = x[i];
+    const T rb = rbt[i], Sb = sbar[i], nb = rhonbar[i];
+    const V3<T> Gb = gbar[i];
+    const uint32_t cnt = nbr_n[i];
     V3<T> xs = zero3<T>();
     for (uint32_t k = 0; k < cnt; ++k) {
         const uint32_t j = nbr[(size_t)k * n + i];
         const V3<T> xij = xi - x[j];
         const Radial<T> R = radial(p, dot(xij, xij));
-        const V3<T> gw = R.gs * xij;
-        V3<T> g = (rb * p.m) * gw;                                      // rho
-        g = g + (p.m) * hess(R, xij, Gb);                               // G
-        g = g + (Sb * p.m * p.m * T(2)) * hess(R, xij, gw);             // S
-        if (R.q < T(1) && R.r >= T(1e-9f)) {                            // near
-            const T wn = T(1) - R.q;
-            g = g + (nb * T(3) * wn * wn * (-p.inv_h) / R.r) * xij;
-        }
-        xs = xs + g;
-        atomic_add3(&xbar[j], -g);
+        xs = xs + density_pair_bar(p, xij, R, rb, Gb, Sb, nb) -
+             density_pair_bar(p, -xij, R, rbt[j], gbar[j], sbar[j], rhonbar[j]);
     }
     const J3<T> J = wall_grad_jac(p, xi);
     xs = xs + jt_mul(J, Gb) + (rb * p.rho0) * fill_grad(p, xi);
-    atomic_add3(&xbar[i], xs);
+    xbar[i] = xbar[i] + xs;
 }
 
 // The gather's adjoint: the adjoints of the cell-ordered inputs go back to
@@ -1110,7 +1174,8 @@ struct AdjImpl : AdjBase {
     // adjoints
     V3<T> *xbar = nullptr, *vbar = nullptr, *abar = nullptr, *bbar = nullptr, *xbar2 = nullptr, *vbar2 = nullptr;
     T *rhobar = nullptr, *rhonbar = nullptr, *alphabar = nullptr, *kdbar = nullptr, *pbar = nullptr,
-      *ppbar = nullptr, *ppbar_next = nullptr;
+      *ppbar = nullptr, *ppbar_next = nullptr, *dbar = nullptr, *rbt = nullptr, *sbar = nullptr;
+    V3<T> *gbar = nullptr;
     double *fbar = nullptr, *cbar = nullptr;
 
     template <class U>
@@ -1225,6 +1290,10 @@ struct AdjImpl : AdjBase {
         AK(alloc(&rhonbar, N));
         AK(alloc(&alphabar, N));
         AK(alloc(&kdbar, N));
+        AK(alloc(&dbar, N));
+        AK(alloc(&rbt, N));
+        AK(alloc(&sbar, N));
+        AK(alloc(&gbar, N));
         AK(alloc(&pbar, N));
         AK(alloc(&ppbar, N));
         AK(alloc(&ppbar_next, N));
@@ -1446,6 +1515,13 @@ struct AdjImpl : AdjBase {
         return FLUID_OK;
     }
 
+    // The density pass reversed: total rho, G and S adjoints, then x.
+    void reverse_density(const V3<T> *xs, const uint32_t *nb, const uint32_t *nbn, const T *rho) {
+        const uint32_t B = nblk(n, kAdjThreads);
+        k_r_density_a<T><<<B, kAdjThreads, 0, stream>>>(mp, n, xs, nb, nbn, rho, rhobar, alphabar, rbt, gbar, sbar);
+        k_r_density_b<T><<<B, kAdjThreads, 0, stream>>>(mp, n, xs, nb, nbn, rbt, gbar, sbar, rhonbar, xbar);
+    }
+
     void reverse_substep(uint32_t k, const Tape<T> &t) {
         const uint32_t B = nblk(n, kAdjThreads), B2 = nblk(n, 256);
         const uint32_t nd = div_it[k], ne = den_it[k];
@@ -1456,13 +1532,13 @@ struct AdjImpl : AdjBase {
         cudaMemsetAsync(rhonbar, 0, sizeof(T) * N, stream);
         cudaMemsetAsync(alphabar, 0, sizeof(T) * N, stream);
         for (uint32_t q = ne; q-- > 0;) {
-            cudaMemsetAsync(kdbar, 0, sizeof(T) * N, stream);
             k_r_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.nbr, t.nbr_n, t.kdden[q], t.wg, vbar,
                                                         kdbar, xbar);
-            k_r_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[q], t.nbr, t.nbr_n, t.rho,
-                                                        t.alpha, t.wg, kdbar, pbar, vbar, xbar, rhobar, alphabar);
+            k_r_kappa_a<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[q], t.nbr, t.nbr_n, t.rho,
+                                                          t.alpha, t.wg, kdbar, pbar, dbar, rhobar, alphabar);
+            k_r_kappa_b<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.vden[q], t.nbr, t.nbr_n, t.wg, dbar, vbar,
+                                                          xbar);
         }
-        cudaMemsetAsync(kdbar, 0, sizeof(T) * N, stream);
         k_r_forces_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, T(xsph), t.x, t.blend, t.nbr, t.nbr_n, t.kdf,
                                                            t.wg, vbar, abar, bbar, kdbar, xbar, fbar + 3 * (size_t)k,
                                                            cbar);
@@ -1470,14 +1546,14 @@ struct AdjImpl : AdjBase {
                                                           t.pp, abar, bbar, kdbar, pbar, xbar, vbar, rhobar, rhonbar,
                                                           ppbar);
         for (uint32_t q = nd; q-- > 0;) {
-            cudaMemsetAsync(kdbar, 0, sizeof(T) * N, stream);
             k_r_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.nbr, t.nbr_n, t.kddiv[q], t.wg, vbar,
                                                         kdbar, xbar);
-            k_r_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[q], t.nbr, t.nbr_n, t.rho,
-                                                        t.alpha, t.wg, kdbar, nullptr, vbar, xbar, rhobar, alphabar);
+            k_r_kappa_a<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[q], t.nbr, t.nbr_n, t.rho,
+                                                          t.alpha, t.wg, kdbar, nullptr, dbar, rhobar, alphabar);
+            k_r_kappa_b<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.vdiv[q], t.nbr, t.nbr_n, t.wg, dbar, vbar,
+                                                          xbar);
         }
-        k_r_density<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.nbr, t.nbr_n, t.rho, rhobar, rhonbar, alphabar,
-                                                      xbar);
+        reverse_density(t.x, t.nbr, t.nbr_n, t.rho);
         // back to the order the substep started from
         k_r_unpermute<T><<<B2, 256, 0, stream>>>(n, t.perm, xbar, vbar, ppbar, xbar2, vbar2, ppbar_next);
         std::swap(xbar, xbar2);
@@ -1501,8 +1577,7 @@ struct AdjImpl : AdjBase {
                                  T(2.0 * (com[2] - target[2]) / n)};
         k_r_loss<T><<<nblk(n, 256), 256, 0, stream>>>(mp, n, fin.rho, gcom, xbar, vbar, rhobar, rhonbar, alphabar,
                                                       ppbar_next);
-        k_r_density<T><<<nblk(n, kAdjThreads), kAdjThreads, 0, stream>>>(mp, n, x, fin.nbr, fin.nbr_n, fin.rho,
-                                                                         rhobar, rhonbar, alphabar, xbar);
+        reverse_density(x, fin.nbr, fin.nbr_n, fin.rho);
         AK(cudaGetLastError());
         const uint32_t nseg = (frames + ce - 1) / ce;
         for (uint32_t q = nseg; q-- > 0;) {
