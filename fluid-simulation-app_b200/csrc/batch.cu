@@ -19,6 +19,7 @@
 // (crates/fluid-core/src/render.rs:1468-1612); this replaces running many
 // of them one after another.
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -70,6 +71,7 @@ struct FluidBatch {
     std::vector<DevParams> P;
     std::vector<uint32_t> first, count, cell_base;
     uint32_t nboxes = 0, n = 0, cells = 0, chunks = 1;
+    uint16_t tpb[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // block size per tuned sweep (0: default)
     int device = 0;
     cudaStream_t stream = nullptr, side = nullptr;
     SimBufs b{};
@@ -96,6 +98,7 @@ struct FluidBatch {
         g.st = cur;
         g.n = n;
         g.nboxes = nboxes;
+        for (int k = 0; k < 8; ++k) g.tpb[k] = tpb[k];
         return g;
     }
     BoxKeys keys() const { return BoxKeys{d_box_of, d_box, d_cell_base, nboxes}; }
@@ -534,6 +537,150 @@ int32_t fluid_batch_get_state(FluidBatch *s, uint32_t box, float *pos4, float *v
     if (prev_p) BK(cudaMemcpy(prev_p, s->b.pp + f, 4 * n, cudaMemcpyDeviceToHost));
     if (temp) BK(cudaMemcpy(temp, s->b.temp + f, 4 * n, cudaMemcpyDeviceToHost));
     if (id) BK(cudaMemcpy(id, s->b.id + f, 4 * n, cudaMemcpyDeviceToHost));
+    return FLUID_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The captured substeps launch with the block sizes of their capture: drop
+// them so the next run captures with the current table.
+void drop_graphs(FluidBatch *s) {
+    cudaStreamSynchronize(s->stream);
+    for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+    s->graphs.clear();
+    if (s->tol_graph) cudaGraphExecDestroy(s->tol_graph);
+    s->tol_graph = nullptr;
+}
+
+// One substep of every box as direct launches at a fixed schedule (one
+// divergence apply, two density pairs) with every tuned sweep at `tpb`,
+// each sweep's launches timed with events: ms[slot] accumulates.
+int32_t timed_substep(FluidBatch *s, int tpb, float *ms, cudaEvent_t *ev) {
+    cudaStream_t st = s->stream;
+    Geo g = s->geo();
+    for (int k = 0; k < kTuneCount; ++k) g.tpb[k] = (uint16_t)tpb;
+    k_clear_acc<<<s->nboxes, 128, 0, st>>>(s->solve);
+    const BoxKeys bk = s->keys();
+    BK(grid_build_enqueue(st, s->b.pos, s->n, GridGeom{}, s->b.keys, s->b.starts, s->b.perm, s->gw, true,
+                          nullptr, nullptr, s->solve, kBatchRing, &bk));
+    launch_gather(st, s->b, s->n);
+    int e = 0;
+    auto timed = [&](int slot, auto &&launch) {
+        cudaEventRecord(ev[e], st);
+        launch();
+        cudaEventRecord(ev[e + 1], st);
+        cudaEventSynchronize(ev[e + 1]);
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, ev[e], ev[e + 1]);
+        ms[slot] += t;
+    };
+    timed(kTuneDensity, [&] { launch_density_div(st, g, s->b, 0); });
+    timed(kTuneApply, [&] { launch_apply(st, g, s->b, false, kGateNone); });
+    timed(kTuneDivKappa, [&] { launch_div_kappa(st, g, s->b, 1, kGateNone); });
+    timed(kTuneForcesEval, [&] { launch_forces_eval(st, g, s->b); });
+    timed(kTuneForcesApply, [&] { launch_forces_apply(st, g, s->b); });
+    for (int k = 0; k < 2; ++k) {
+        timed(kTuneDenKappa, [&] { launch_den_kappa(st, g, s->b, k, kGateNone); });
+        timed(kTuneApply, [&] { launch_apply(st, g, s->b, true, kGateNone); });
+    }
+    timed(kTuneIntegrate, [&] { launch_integrate(st, g, s->b, 0, 1, 1, 2); });
+    BK(cudaGetLastError());
+    return FLUID_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t fluid_batch_set_blocks(FluidBatch *s, const uint32_t *tpb) {
+    if (!s || !tpb) return report_error(FLUID_ERR_ARG, "null argument");
+    for (int k = 0; k < kTuneCount; ++k)
+        if (tpb[k] != 0 && tpb[k] != 64 && tpb[k] != 128 && tpb[k] != 256)
+            return report_error(FLUID_ERR_ARG, "block sizes are 64, 128 or 256 (0: default)");
+    BK(cudaSetDevice(s->device));
+    drop_graphs(s);
+    for (int k = 0; k < kTuneCount; ++k) s->tpb[k] = (uint16_t)tpb[k];
+    return FLUID_OK;
+}
+
+int32_t fluid_batch_get_blocks(const FluidBatch *s, uint32_t *tpb) {
+    if (!s || !tpb) return report_error(FLUID_ERR_ARG, "null argument");
+    for (int k = 0; k < kTuneCount; ++k) tpb[k] = s->tpb[k];
+    return FLUID_OK;
+}
+
+int32_t fluid_batch_autotune(FluidBatch *s, const FluidStep *steps, uint32_t *chosen, float *ms_out) {
+    if (!s || !steps) return report_error(FLUID_ERR_ARG, "null argument");
+    const size_t nb = s->nboxes, n = s->n;
+    for (size_t k = 0; k < nb; ++k)
+        if (!(steps[k].dt > 0.0f) || !std::isfinite(steps[k].dt))
+            return report_error(FLUID_ERR_ARG, "batch steps need a finite dt > 0");
+    BK(cudaSetDevice(s->device));
+    BK(cudaStreamSynchronize(s->stream));
+    // the Step blocks of the timed substeps go straight to the current slots
+    std::vector<DevStep> d(nb);
+    for (size_t k = 0; k < nb; ++k) host_step_constants(s->cfg[k].xsph_blend, steps[k], d[k]);
+    // snapshot of everything a substep changes that outlives it
+    std::vector<void *> tmp;
+    auto save = [&](const void *src, size_t bytes) -> void * {
+        void *q = nullptr;
+        if (cudaMalloc(&q, bytes) != cudaSuccess) return nullptr;
+        tmp.push_back(q);
+        cudaMemcpyAsync(q, src, bytes, cudaMemcpyDeviceToDevice, s->stream);
+        return q;
+    };
+    struct Saved {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    std::vector<Saved> saved = {{s->b.pos, nullptr, 16 * n}, {s->b.vel, nullptr, 16 * n},
+                                {s->b.pvel, nullptr, 16 * n}, {s->b.pp, nullptr, 4 * n},
+                                {s->b.temp, nullptr, 4 * n},  {s->b.id, nullptr, 4 * n},
+                                {s->solve, nullptr, nb * sizeof(DevSolve)}, {s->cur, nullptr, nb * sizeof(DevStep)}};
+    int32_t rc = FLUID_OK;
+    for (auto &v : saved) {
+        v.src = save(v.dst, v.bytes);
+        if (!v.src) rc = report_error(FLUID_ERR_OOM, "autotune: no room for the state snapshot");
+    }
+    auto restore = [&] {
+        for (auto &v : saved)
+            if (v.src) cudaMemcpyAsync(v.dst, v.src, v.bytes, cudaMemcpyDeviceToDevice, s->stream);
+    };
+    const int cand[3] = {64, 128, 256};
+    float ms[3][kTuneCount] = {};
+    cudaEvent_t ev[2];
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    for (int c = 0; c < 3 && rc == FLUID_OK; ++c) {
+        for (int rep = 0; rep < 2 && rc == FLUID_OK; ++rep) {  // the first run warms up
+            restore();
+            cudaMemcpyAsync(s->cur, d.data(), nb * sizeof(DevStep), cudaMemcpyHostToDevice, s->stream);
+            float t[kTuneCount] = {};
+            rc = timed_substep(s, cand[c], t, ev);
+            if (rep == 1)
+                for (int k = 0; k < kTuneCount; ++k) ms[c][k] = t[k];
+        }
+    }
+    restore();
+    cudaStreamSynchronize(s->stream);
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    for (void *q : tmp) cudaFree(q);
+    if (rc != FLUID_OK) return rc;
+    BK(cudaGetLastError());
+    drop_graphs(s);
+    for (int k = 0; k < kTuneCount; ++k) {
+        int best = 1;
+        for (int c = 0; c < 3; ++c)
+            if (ms[c][k] < ms[best][k]) best = c;
+        s->tpb[k] = (uint16_t)cand[best];
+        if (chosen) chosen[k] = (uint32_t)cand[best];
+        if (ms_out)
+            for (int c = 0; c < 3; ++c) ms_out[c * kTuneCount + k] = ms[c][k];
+    }
     return FLUID_OK;
 }
 

@@ -423,11 +423,11 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
     return found;
 }
 
-template <bool kB>
-__global__ void __launch_bounds__(kSolveThreads) k_density_div(Geo g, SimBufs b, int slot) {
-    __shared__ uint16_t s_hit[kStage][kSolveThreads];
-    __shared__ uint32_t s_beg[9][kSolveThreads];
-    __shared__ uint32_t s_end[9][kSolveThreads];
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB) k_density_div(Geo g, SimBufs b, int slot) {
+    __shared__ uint16_t s_hit[kStage][TPB];
+    __shared__ uint32_t s_beg[9][TPB];
+    __shared__ uint32_t s_end[9][TPB];
     const uint32_t n = g.n;
     const uint32_t tid = threadIdx.x;
     const uint32_t i = blockIdx.x * blockDim.x + tid;
@@ -557,8 +557,8 @@ __device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
 // ---- divergence predictor for a later divergence iteration ---------------
 // density_div's divergence sums again over the list, with this
 // iteration's velocities.
-template <bool kB>
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_div_kappa(Geo g, SimBufs b, int slot,
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_div_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -603,8 +603,8 @@ __device__ __forceinline__ F3 kappa_sum(const SimBufs &b, uint32_t i, uint32_t n
 // ---- apply_kappa_wide: div_apply / den_apply (sim_solve.wgsl:608-621) -----
 // For the density iterations the applied pressure k*rho that den_kappa held
 // back joins the pressure here, with the kappa it belongs to.
-template <bool kB>
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure,
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure,
                                                                    int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -624,8 +624,8 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_apply(Geo g, SimBuf
 }
 
 // ---- forces_eval (sim_solve.wgsl:524-592) ---------------------------------
-template <bool kB>
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_eval(Geo g, SimBufs b) {
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_eval(Geo g, SimBufs b) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -706,8 +706,8 @@ __device__ __forceinline__ F3 fingers(const FluidStep &st, F3 pos, F3 v) {
 }
 
 // ---- forces_den_apply (sim_solve.wgsl:630-663) -----------------------------
-template <bool kB>
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_apply(Geo g, SimBufs b) {
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_apply(Geo g, SimBufs b) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -735,8 +735,8 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_forces_apply(Geo g,
 }
 
 // ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
-template <bool kB>
-__global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(Geo g, SimBufs b, int slot,
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_den_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -772,8 +772,8 @@ __global__ void __launch_bounds__(kSolveThreads, FCU_MINB) k_den_kappa(Geo g, Si
 // With div_slot >= 0 (the fixed schedule) each box's first slot also records
 // the box's residuals from the accumulator slots of the last divergence and
 // density predictions, and the iteration counts.
-template <bool kB>
-__global__ void __launch_bounds__(256) k_integrate(Geo g, SimBufs b, int div_slot, int den_slot,
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB) k_integrate(Geo g, SimBufs b, int div_slot, int den_slot,
                                                    int div_iters, int den_iters) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1097,37 +1097,46 @@ void launch_gather(cudaStream_t s, const SimBufs &b, uint32_t n) {
 }
 
 // One launch of `kern` over g.n particles: the batch instance when the
-// geometry has a box map, the one-box instance otherwise.
-#define FCU_SWEEP(kern, threads, ...)                                                   \
+// geometry has a box map, the one-box instance otherwise, at the block size
+// the geometry's tuning table holds for the kernel (or the default).
+#define FCU_SWEEP_AT(kern, T, ...)                                                      \
     do {                                                                                \
-        const uint32_t blocks_ = blocks_for(g.n, threads);                              \
-        if (!blocks_) return;                                                           \
-        if (g.box_of) kern<true><<<blocks_, threads, 0, s>>>(__VA_ARGS__);              \
-        else kern<false><<<blocks_, threads, 0, s>>>(__VA_ARGS__);                      \
+        const uint32_t blocks_ = blocks_for(g.n, T);                                    \
+        if (g.box_of) kern<true, T><<<blocks_, T, 0, s>>>(__VA_ARGS__);                 \
+        else kern<false, T><<<blocks_, T, 0, s>>>(__VA_ARGS__);                         \
+    } while (0)
+#define FCU_SWEEP(kern, slot_id, deflt, ...)                                            \
+    do {                                                                                \
+        if (!g.n) return;                                                               \
+        const int tpb_ = g.tpb[slot_id] ? (int)g.tpb[slot_id] : (deflt);                \
+        if (tpb_ == 64) FCU_SWEEP_AT(kern, 64, __VA_ARGS__);                            \
+        else if (tpb_ == 256) FCU_SWEEP_AT(kern, 256, __VA_ARGS__);                     \
+        else FCU_SWEEP_AT(kern, 128, __VA_ARGS__);                                      \
     } while (0)
 
 void launch_density_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot) {
-    FCU_SWEEP(k_density_div, kSolveThreads, g, b, slot);
+    FCU_SWEEP(k_density_div, kTuneDensity, kSolveThreads, g, b, slot);
 }
 void launch_div_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
-    FCU_SWEEP(k_div_kappa, kSolveThreads, g, b, slot, gate);
+    FCU_SWEEP(k_div_kappa, kTuneDivKappa, kSolveThreads, g, b, slot, gate);
 }
 void launch_apply(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int gate) {
-    FCU_SWEEP(k_apply, kSolveThreads, g, b, add_pressure ? 1 : 0, gate);
+    FCU_SWEEP(k_apply, kTuneApply, kSolveThreads, g, b, add_pressure ? 1 : 0, gate);
 }
 void launch_forces_eval(cudaStream_t s, const Geo &g, const SimBufs &b) {
-    FCU_SWEEP(k_forces_eval, kSolveThreads, g, b);
+    FCU_SWEEP(k_forces_eval, kTuneForcesEval, kSolveThreads, g, b);
 }
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b) {
-    FCU_SWEEP(k_forces_apply, kSolveThreads, g, b);
+    FCU_SWEEP(k_forces_apply, kTuneForcesApply, kSolveThreads, g, b);
 }
 void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
-    FCU_SWEEP(k_den_kappa, kSolveThreads, g, b, slot, gate);
+    FCU_SWEEP(k_den_kappa, kTuneDenKappa, kSolveThreads, g, b, slot, gate);
 }
 void launch_integrate(cudaStream_t s, const Geo &g, const SimBufs &b, int div_slot, int den_slot,
                       int div_iters, int den_iters) {
-    FCU_SWEEP(k_integrate, 256, g, b, div_slot, den_slot, div_iters, den_iters);
+    FCU_SWEEP(k_integrate, kTuneIntegrate, 256, g, b, div_slot, den_slot, div_iters, den_iters);
 }
+#undef FCU_SWEEP_AT
 #undef FCU_SWEEP
 
 void launch_tol_finish(cudaStream_t s, const Geo &g, int which, int first, float tol,

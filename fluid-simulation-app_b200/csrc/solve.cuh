@@ -39,11 +39,26 @@ struct SimBufs {
     float *stats;       // [box][16]
 };
 
+// The sweeps whose block size can be tuned (entries of Geo::tpb).
+enum TuneSlot : int {
+    kTuneDensity = 0,
+    kTuneDivKappa,
+    kTuneApply,
+    kTuneForcesEval,
+    kTuneForcesApply,
+    kTuneDenKappa,
+    kTuneIntegrate,
+    kTuneCount
+};
+
 // Which box a slot belongs to, and the per-box constants, Step blocks and
 // solver counters. One box: box_of is null, the constants travel by value
 // in `one` (the kernel's parameter space), solve and st point at one entry.
-// A batch: box_of, box, cell_base and first are device arrays.
+// A batch: box_of, box, cell_base and first are device arrays. tpb: the
+// launch's block size per tuned sweep (64, 128 or 256; 0 = the default),
+// read by the host-side launchers only.
 struct Geo {
+    uint16_t tpb[8];
     DevParams one;                           // the box, when there is one
     const DevParams *__restrict__ box;       // [nboxes] (batch)
     const uint16_t *__restrict__ box_of;     // [n] (batch) or null

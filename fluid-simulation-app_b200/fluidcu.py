@@ -160,6 +160,9 @@ def lib():
         "fluid_batch_stats": (i32, [P, C.POINTER(FluidSimStats)]),
         "fluid_batch_sync": (i32, [P]),
         "fluid_batch_get_state": (i32, [P, u32, vp, vp, vp, vp, vp, vp]),
+        "fluid_batch_autotune": (i32, [P, C.POINTER(FluidStep), vp, vp]),
+        "fluid_batch_set_blocks": (i32, [P, vp]),
+        "fluid_batch_get_blocks": (i32, [P, vp]),
         "fluid_adjoint_create": (P, [C.POINTER(FluidSimConfig), u32, u32, f, f, u32, u32]),
         "fluid_adjoint_destroy": (None, [P]),
         "fluid_adjoint_count": (u32, [P]),
@@ -344,6 +347,27 @@ class Batch:
 
     def stream(self):
         return lib().fluid_batch_stream(self.h)
+
+    TUNED = ("density_div", "div_kappa", "apply", "forces_eval", "forces_apply", "den_kappa",
+             "integrate")
+
+    def autotune(self, steps):
+        """Block size per tuned sweep from one timed substep per candidate
+        (64/128/256) of `steps` (nboxes FluidStep); the state is restored."""
+        arr = (FluidStep * self.nboxes)(*steps)
+        chosen = np.zeros(7, np.uint32)
+        ms = np.zeros((3, 7), np.float32)
+        check(lib().fluid_batch_autotune(self.h, arr, _p(chosen), _p(ms)), "batch_autotune")
+        return dict(zip(self.TUNED, chosen.tolist())), ms
+
+    def set_blocks(self, tpb):
+        a = np.ascontiguousarray(tpb, np.uint32)
+        check(lib().fluid_batch_set_blocks(self.h, _p(a)), "batch_set_blocks")
+
+    def blocks(self):
+        a = np.zeros(7, np.uint32)
+        check(lib().fluid_batch_get_blocks(self.h, _p(a)), "batch_get_blocks")
+        return a
 
     def stats(self, allow_error=False):
         arr = (FluidSimStats * self.nboxes)()

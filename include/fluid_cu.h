@@ -341,6 +341,22 @@ int32_t fluid_batch_sync(FluidBatch *batch);
 int32_t fluid_batch_get_state(FluidBatch *batch, uint32_t box, float *pos4, float *vel4,
                               float *prev_vel4, float *prev_p, float *temp, uint32_t *id);
 
+/* The tuned sweeps, in this order, for the block-size calls below: density,
+ * divergence prediction, apply, forces, forces apply, density prediction,
+ * integrate. */
+#define FLUID_TUNED_SWEEPS 7
+/* Chooses each tuned sweep's block size (64, 128 or 256 threads) by timing
+ * one substep of every candidate, Step blocks steps[nboxes], on the batch's
+ * current state, which is restored afterwards (the batch does not advance).
+ * Later substeps launch with the choices; results do not depend on them.
+ * chosen[7] receives the sizes and ms[3][7] the times (candidate-major),
+ * either may be null. Synchronises; allocates a snapshot of the state. */
+int32_t fluid_batch_autotune(FluidBatch *batch, const FluidStep *steps, uint32_t *chosen,
+                             float *ms);
+/* Sets (0: the default) or reads the block size of each tuned sweep. */
+int32_t fluid_batch_set_blocks(FluidBatch *batch, const uint32_t *tpb);
+int32_t fluid_batch_get_blocks(const FluidBatch *batch, uint32_t *tpb);
+
 /* ---- the adjoint -----------------------------------------------------------
  * A differentiable model of the substep (density, divergence solve, forces,
  * density solve, advection; particles in a fixed order, neighbour lists

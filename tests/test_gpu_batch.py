@@ -90,6 +90,41 @@ def test_batched_fixed_schedule_matches_the_oracle_and_stats(fcu, orc, wl):
         assert stats[b].density_min == np.float32(o[2]) and stats[b].density_max == np.float32(o[3]), b
 
 
+def test_block_sizes_and_the_autotuner_change_no_bit(fcu, wl):
+    # The sweeps' block size only regroups threads: every box stays
+    # bit-identical at 64, 128 and 256 threads, and the autotuner's timed
+    # substeps leave the batch where it was.
+    nb = 4
+    cfgs = small_boxes(fcu, wl, nb)
+    steps = wl.batched_frame_steps(fcu, nb, frames=3, substeps=4, seed=9)
+    ref = fcu.Batch(cfgs)
+    ref.run(steps)
+    for tpb in (64, 256):
+        other = fcu.Batch(cfgs)
+        other.set_blocks([tpb] * 7)
+        assert list(other.blocks()) == [tpb] * 7
+        other.run(steps)
+        for b in range(nb):
+            a, c = ref.state(b), other.state(b)
+            for k in ("pos", "vel", "prev_vel", "prev_p", "temp", "id"):
+                assert_same_bits(a[k], c[k], f"{tpb} threads box {b} {k}")
+    tuned = fcu.Batch(cfgs)
+    tuned.run(steps[:4])
+    before = [tuned.state(b) for b in range(nb)]
+    chosen, ms = tuned.autotune(steps[4])
+    assert set(chosen.values()) <= {64, 128, 256} and np.all(ms > 0)
+    for b in range(nb):
+        after = tuned.state(b)
+        for k in ("pos", "vel", "prev_vel", "prev_p", "temp", "id"):
+            assert_same_bits(before[b][k], after[k], f"autotune restores box {b} {k}")
+    assert tuned.stats()[0].substeps == 4
+    tuned.run(steps[4:])
+    for b in range(nb):
+        a, c = ref.state(b), tuned.state(b)
+        for k in ("pos", "vel", "prev_vel", "prev_p", "temp", "id"):
+            assert_same_bits(a[k], c[k], f"tuned box {b} {k}")
+
+
 def test_a_batch_of_one_is_the_one_box_simulation(fcu, wl):
     cfg = small_boxes(fcu, wl, 1)[0]
     batch = fcu.Batch([cfg])
