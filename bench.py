@@ -351,6 +351,9 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     nw = BATCH_WARMUP_FRAMES * SUBSTEPS_PER_FRAME
     batch.run(steps[:nw])
     batch.sync()
+    # block sizes from the autotuner (one timed substep per candidate on the
+    # warmed-up state, which it restores)
+    chosen, tune_ms = batch.autotune(steps[nw])
     before = batch.stats()
     stream = torch.cuda.ExternalStream(batch.stream())
     if world > 1:
@@ -386,7 +389,10 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
             "mean_div_iters_per_box": float(rows[:, 1].mean() / sub),
             "compression_avg_mean": float(rows[:, 2].mean()),
             "compression_avg_worst_box": float(rows[:, 2].max()),
-            "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu}
+            "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu,
+            "autotuned_blocks": chosen,
+            "autotune_ms_by_block": {str(t): dict(zip(fcu.Batch.TUNED, [round(float(x), 4) for x in tune_ms[c]]))
+                                     for c, t in enumerate((64, 128, 256))}}
 
 
 ADJ_FRAMES = 120
