@@ -191,6 +191,12 @@ uint32_t fluid_substep_floor(float dt, float dt_sub_max) {  // render.rs:63-65
 
 uint32_t fluid_refine_passes(float dt_sub) { return dt_sub > kRefineShortDt ? 5u : 2u; }  // :76-78
 
+float fluid_field_keep_target(float v_max) {  // render.rs:1107-1111, FIELD_KEEP :517
+    float t = (v_max - 0.05f) / 0.20f;
+    t = t < 0.0f ? 0.0f : (t > 1.0f ? 1.0f : t);
+    return 0.8f * (1.0f - t * t * (3.0f - 2.0f * t));
+}
+
 uint32_t fluid_substeps_for(float dt, float v_max, float spacing, uint32_t cap) {  // :97-106
     uint32_t n = sat_u32f(std::ceil(dt * v_max / (0.4f * spacing)));
     const uint32_t fl = fluid_substep_floor(dt, kSubstepPerSpacing * spacing);

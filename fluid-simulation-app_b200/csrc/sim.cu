@@ -15,6 +15,7 @@
 #include <utility>
 #include <vector>
 
+#include "field.cuh"
 #include "grid.cuh"
 #include "solve.cuh"
 
@@ -120,6 +121,11 @@ struct FluidSim {
     cudaEvent_t stats_ready = nullptr;
     bool stats_pending = false;
     float v_max_stale = 0.0f;
+    // the render-side thickness field (fluid_sim_field_*), allocated on use
+    float2 *field = nullptr;
+    float4 *field_filtered = nullptr;
+    unsigned long long *field_acc = nullptr;
+    FieldGeom fgeom{};
 
     // The sweeps' view of this one-box simulation.
     Geo geo() const {
@@ -599,6 +605,9 @@ void fluid_sim_destroy(FluidSim *s) {
     if (s->h_ring) cudaFreeHost(s->h_ring);
     if (s->h_stats_stale) cudaFreeHost(s->h_stats_stale);
     if (s->stats_ready) cudaEventDestroy(s->stats_ready);
+    if (s->field) cudaFree(s->field);
+    if (s->field_filtered) cudaFree(s->field_filtered);
+    if (s->field_acc) cudaFree(s->field_acc);
     if (s->side) cudaStreamDestroy(s->side);
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -902,6 +911,71 @@ int32_t fluid_sim_set_tracers(FluidSim *s, const uint32_t *packed2) {
     CK(cudaSetDevice(s->device));
     CK(cudaStreamSynchronize(s->stream));
     if (s->ntr) CK(cudaMemcpy(s->b.tracers, packed2, 8ull * s->ntr, cudaMemcpyHostToDevice));
+    return FLUID_OK;
+}
+
+// sim_sprites.wgsl body + weight and the field pass of render.rs:3233-3282:
+// the decay draw (field *= keep) and one splat of every particle at blend
+// constant 1 - keep, into the handle's float2 field.
+int32_t fluid_sim_field_splat(FluidSim *s, const FluidFieldParams *p) {
+    if (!s || !p) return fail(FLUID_ERR_ARG, "null argument");
+    if (p->width == 0 || p->height == 0 || (uint64_t)p->width * p->height > (1ull << 26))
+        return fail(FLUID_ERR_ARG, "field size must be 1..2^26 texels");
+    if (!(p->keep >= 0.0f && p->keep <= 1.0f)) return fail(FLUID_ERR_ARG, "keep must be in [0, 1]");
+    if (p->lens > 4u) return fail(FLUID_ERR_ARG, "lens codes are 0..4");
+    if (p->lens && !(p->hi != p->lo)) return fail(FLUID_ERR_ARG, "the lens ramp needs hi != lo");
+    CK(cudaSetDevice(s->device));
+    const size_t texels = (size_t)p->width * p->height;
+    if (!s->field || s->fgeom.w != p->width || s->fgeom.h != p->height) {
+        CK(cudaStreamSynchronize(s->stream));
+        if (s->field) cudaFree(s->field);
+        if (s->field_filtered) cudaFree(s->field_filtered);
+        if (s->field_acc) cudaFree(s->field_acc);
+        s->field = nullptr;
+        s->field_filtered = nullptr;
+        s->field_acc = nullptr;
+        CK(cudaMalloc(&s->field, texels * sizeof(float2)));
+        CK(cudaMalloc(&s->field_filtered, texels * sizeof(float4)));
+        CK(cudaMalloc(&s->field_acc, texels * 2 * sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(s->field, 0, texels * sizeof(float2), s->stream));
+        CK(cudaMemsetAsync(s->field_filtered, 0, texels * sizeof(float4), s->stream));
+        CK(cudaMemsetAsync(s->field_acc, 0, texels * 2 * sizeof(unsigned long long), s->stream));
+    }
+    FieldGeom &g = s->fgeom;
+    g.cx = s->P.tracer_c[0];  // the slab's extent -(box_min + cell), or the box's centre and half size
+    g.cy = s->P.tracer_c[1];
+    g.ex = s->P.tracer_e[0];
+    g.ey = s->P.tracer_e[1];
+    g.radius = s->P.h * 1.5f;  // SPLAT_RADIUS, sim_sprites.wgsl
+    g.w = p->width;
+    g.h = p->height;
+    g.lens = p->lens;
+    g.lo = p->lo;
+    g.hi = p->hi;
+    launch_field_splat(s->stream, g, s->b.pos, s->b.vel, s->b.pvel, s->b.density, s->n, p->keep, 1.0f - p->keep,
+                       s->field, s->field_acc);
+    CK(cudaGetLastError());
+    return FLUID_OK;
+}
+
+// sim_surface.wgsl field_filter over the current field.
+int32_t fluid_sim_field_filter(FluidSim *s) {
+    if (!s) return fail(FLUID_ERR_ARG, "null handle");
+    if (!s->field) return fail(FLUID_ERR_STATE, "no field yet: splat first");
+    CK(cudaSetDevice(s->device));
+    launch_field_filter(s->stream, s->fgeom, s->field, s->field_filtered);
+    CK(cudaGetLastError());
+    return FLUID_OK;
+}
+
+int32_t fluid_sim_field_read(FluidSim *s, float *field2, float *filtered4) {
+    if (!s) return fail(FLUID_ERR_ARG, "null handle");
+    if (!s->field) return fail(FLUID_ERR_STATE, "no field yet: splat first");
+    CK(cudaSetDevice(s->device));
+    CK(cudaStreamSynchronize(s->stream));
+    const size_t texels = (size_t)s->fgeom.w * s->fgeom.h;
+    if (field2) CK(cudaMemcpy(field2, s->field, texels * sizeof(float2), cudaMemcpyDeviceToHost));
+    if (filtered4) CK(cudaMemcpy(filtered4, s->field_filtered, texels * sizeof(float4), cudaMemcpyDeviceToHost));
     return FLUID_OK;
 }
 

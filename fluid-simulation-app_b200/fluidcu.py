@@ -81,6 +81,11 @@ class FluidGrid(C.Structure):
     _fields_ = [("min", C.c_float * 3), ("cell", C.c_float), ("dims", C.c_uint32 * 3)]
 
 
+class FluidFieldParams(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("keep", C.c_float),
+                ("lens", C.c_uint32), ("lo", C.c_float), ("hi", C.c_float)]
+
+
 class FluidMotion(C.Structure):
     _fields_ = [("gravity", FluidVec3), ("user_acceleration", FluidVec3),
                 ("rotation_rate", FluidVec3)]
@@ -140,6 +145,10 @@ def lib():
         "fluid_sim_get_tracers": (i32, [P, vp]),
         "fluid_sim_set_tracers": (i32, [P, vp]),
         "fluid_sim_read_field": (i32, [P, i32, vp, u64]),
+        "fluid_sim_field_splat": (i32, [P, C.POINTER(FluidFieldParams)]),
+        "fluid_sim_field_filter": (i32, [P]),
+        "fluid_sim_field_read": (i32, [P, vp, vp]),
+        "fluid_field_keep_target": (f, [f]),
         "fluid_sim_profile_step": (i32, [P, C.POINTER(FluidStep), C.POINTER(f),
                                          C.POINTER(C.c_char_p), u32]),
         "fluid_sim_kernels_per_substep": (u32, [P]),
@@ -483,6 +492,21 @@ class Sim:
     def set_tracers(self, packed):
         packed = np.ascontiguousarray(packed, np.uint32)
         check(lib().fluid_sim_set_tracers(self.h, _p(packed)), "set_tracers")
+
+    def field_splat(self, width, height, keep=0.0, lens=0, lo=0.0, hi=1.0):
+        p = FluidFieldParams(width, height, keep, lens, lo, hi)
+        self._field_shape = (height, width)
+        return check(lib().fluid_sim_field_splat(self.h, C.byref(p)), "field_splat")
+
+    def field_filter(self):
+        return check(lib().fluid_sim_field_filter(self.h), "field_filter")
+
+    def field_read(self):
+        h, w = self._field_shape
+        f2 = np.zeros((h, w, 2), np.float32)
+        f4 = np.zeros((h, w, 4), np.float32)
+        check(lib().fluid_sim_field_read(self.h, _p(f2), _p(f4)), "field_read")
+        return f2, f4
 
     def field(self, name):
         n = self.n

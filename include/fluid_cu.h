@@ -308,6 +308,32 @@ int32_t fluid_sim_profile_step(FluidSim *sim, const FluidStep *step, float *ms,
 /* Kernel launches one substep issues at the current schedule (fixed mode). */
 uint32_t fluid_sim_kernels_per_substep(const FluidSim *sim);
 
+/* ---- the render-side thickness field ---------------------------------------
+ * The body splat of sim_sprites.wgsl (`body`, `weight`, radius 1.5 h, an
+ * orthographic view of the box's x-y extent) with the decay draw of the
+ * field pass (render.rs:3233-3282), and sim_surface.wgsl `field_filter`,
+ * as CUDA into device buffers the handle owns: no graphics stack. */
+typedef struct FluidFieldParams {
+    uint32_t width, height; /* texels (the reference uses a quarter of the drawable per axis) */
+    float keep;             /* fraction of the previous field kept (0: a fresh splat) */
+    uint32_t lens;          /* g channel: 0 none, 1 accel lens, 2 pressure lens, 3 density, 4 speed */
+    float lo, hi;           /* the lens ramp's ends (sim_sprites.wgsl lens_at) */
+} FluidFieldParams;
+
+/* field = field * keep + (1 - keep) * splat of every particle: r the
+ * thickness, g the thickness weighted by the lens. (Re)allocates and zeroes
+ * the field when its size changes. Asynchronous. */
+int32_t fluid_sim_field_splat(FluidSim *sim, const FluidFieldParams *p);
+/* field_filter of the current field: (blurred thickness, x difference,
+ * y difference, Laplacian) per texel. Asynchronous. */
+int32_t fluid_sim_field_filter(FluidSim *sim);
+/* Reads the field [height][width][2] and the filtered field
+ * [height][width][4] (either may be null). Synchronises. */
+int32_t fluid_sim_field_read(FluidSim *sim, float *field2, float *filtered4);
+/* The field's keep fraction for a v_max (render.rs:1107-1111): 0.8 at rest,
+ * down to 0 across 0.05-0.25 m/s. */
+float fluid_field_keep_target(float v_max);
+
 /* ---- batched boxes --------------------------------------------------------
  * Many independent boxes stepped by the same launches: each kernel of a
  * substep covers every box, a substep is one graph launch, and in the

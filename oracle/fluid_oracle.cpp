@@ -1340,4 +1340,104 @@ void or_sim_field(const OrSim *s, int field, void *out) {
     }
 }
 
+
+
+// ---- the render-side thickness field ------------------------------------------
+
+static float or_clampf(float e, float lo, float hi) { return std::fmin(std::fmax(e, lo), hi); }
+
+// sim_sprites.wgsl lens_at
+static float or_lens_value(uint32_t lens, const float *v, const float *pv, float rho, float lo, float hi) {
+    float m;
+    switch (lens) {
+    case 1u: m = v[3]; break;
+    case 2u: m = pv[3]; break;
+    case 3u: m = rho; break;
+    default: m = std::sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]); break;
+    }
+    return or_clampf((m - lo) / (hi - lo), 0.0f, 1.0f);
+}
+
+// Weights summed as 2^-20 fixed-point integers (order-free), then the decay
+// and the blend constant per texel in FP32.
+void or_field_splat(const float *pos4, const float *vel4, const float *pvel4, const float *density,
+                    uint32_t n, const float geom[7], uint32_t w, uint32_t h, uint32_t lens, float keep,
+                    float *field2) {
+    const float gcx = geom[0], gcy = geom[1], ex = geom[2], ey = geom[3], radius = geom[4];
+    const float lo = geom[5], hi = geom[6];
+    const double scale = 1048576.0;
+    std::vector<unsigned long long> acc(2 * (size_t)w * h, 0ull);
+    const float W = (float)w, H = (float)h;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *p = &pos4[4 * (size_t)i];
+        const float px = (p[0] - gcx) / ex, py = (p[1] - gcy) / ey;
+        const float rx = radius / ex, ry = radius / ey;
+        int tx0 = (int)std::floor((px - rx + 1.0f) * 0.5f * W - 0.5f) - 1;
+        int tx1 = (int)std::ceil((px + rx + 1.0f) * 0.5f * W - 0.5f) + 1;
+        int ty0 = (int)std::floor((1.0f - (py + ry)) * 0.5f * H - 0.5f) - 1;
+        int ty1 = (int)std::ceil((1.0f - (py - ry)) * 0.5f * H - 0.5f) + 1;
+        tx0 = tx0 < 0 ? 0 : tx0;
+        ty0 = ty0 < 0 ? 0 : ty0;
+        tx1 = tx1 > (int)w - 1 ? (int)w - 1 : tx1;
+        ty1 = ty1 > (int)h - 1 ? (int)h - 1 : ty1;
+        const float lv = lens ? or_lens_value(lens, &vel4[4 * (size_t)i], &pvel4[4 * (size_t)i], density[i], lo, hi)
+                              : 0.0f;
+        for (int ty = ty0; ty <= ty1; ++ty) {
+            const float yt = 1.0f - ((float)ty + 0.5f) / H * 2.0f;
+            const float cy = (yt - py) / ry;
+            for (int tx = tx0; tx <= tx1; ++tx) {
+                const float xt = ((float)tx + 0.5f) / W * 2.0f - 1.0f;
+                const float cx = (xt - px) / rx;
+                const float falloff = std::fmax(1.0f - (cx * cx + cy * cy), 0.0f);
+                const float wt = falloff * falloff * 0.5f;
+                if (wt > 0.0f) {
+                    unsigned long long *a = &acc[2 * ((size_t)ty * w + tx)];
+                    a[0] += (unsigned long long)std::llrint((double)wt * scale);
+                    if (lens) a[1] += (unsigned long long)std::llrint((double)(wt * lv) * scale);
+                }
+            }
+        }
+    }
+    const float splat = 1.0f - keep;
+    for (size_t t = 0; t < (size_t)w * h; ++t) {
+        const float r = (float)((double)acc[2 * t] / scale);
+        const float g = (float)((double)acc[2 * t + 1] / scale);
+        field2[2 * t] = field2[2 * t] * keep + splat * r;
+        field2[2 * t + 1] = field2[2 * t + 1] * keep + splat * g;
+    }
+}
+
+// The tile computation of field_filter written per texel: H blurs along x
+// over edge-clamped taps, V blurs H along y, and the differences take V at
+// the four neighbours (which may lie one texel past the edge, as the tile's
+// apron does).
+void or_field_filter(const float *field2, uint32_t w, uint32_t h, float ex, float ey, float *out4) {
+    const float B[4] = {0.3125f, 0.234375f, 0.09375f, 0.015625f};
+    auto cl = [](int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); };
+    auto raw = [&](int x, int y) { return field2[2 * ((size_t)cl(y, (int)h - 1) * w + cl(x, (int)w - 1))]; };
+    auto hblur = [&](int x, int y) {
+        float a = raw(x, y) * B[0];
+        for (int k = 1; k <= 3; ++k) a += (raw(x + k, y) + raw(x - k, y)) * B[k];
+        return a;
+    };
+    auto vblur = [&](int x, int y) {
+        float a = hblur(x, y) * B[0];
+        for (int k = 1; k <= 3; ++k) a += (hblur(x, y + k) + hblur(x, y - k)) * B[k];
+        return a;
+    };
+    const float sx = 2.0f * ex / (float)w, sy = 2.0f * ey / (float)h;
+    const float aspect = (sx * sx) / (sy * sy);
+    for (int y = 0; y < (int)h; ++y)
+        for (int x = 0; x < (int)w; ++x) {
+            const float d = vblur(x, y), xp = vblur(x + 1, y), xm = vblur(x - 1, y);
+            const float yp = vblur(x, y + 1), ym = vblur(x, y - 1);
+            const float lap = (xp + xm - 2.0f * d) + (yp + ym - 2.0f * d) * aspect;
+            float *o = &out4[4 * ((size_t)y * w + x)];
+            o[0] = d;
+            o[1] = xp - xm;
+            o[2] = ym - yp;
+            o[3] = lap;
+        }
+}
+
 }  // extern "C"

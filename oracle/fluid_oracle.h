@@ -160,6 +160,18 @@ enum {
 };
 void or_sim_field(const OrSim *s, int field, void *out);
 
+/* The render-side thickness field. geom = {cx, cy, ex, ey, radius, lo, hi}:
+ * the field spans world x in cx +- ex, y in cy +- ey. The body splat of
+ * sim_sprites.wgsl (`body`, `weight`, `lens_at`; lens 0 none, 1 accel lens,
+ * 2 pressure lens, 3 density, 4 speed) with the decay draw of render.rs:
+ * 3233-3282: field2[h][w][2] = field2 * keep + (1 - keep) * splat. */
+void or_field_splat(const float *pos4, const float *vel4, const float *pvel4, const float *density,
+                    uint32_t n, const float geom[7], uint32_t w, uint32_t h, uint32_t lens, float keep,
+                    float *field2);
+/* sim_surface.wgsl field_filter: out4[h][w] = (blurred, x difference,
+ * y difference, Laplacian) of field2's thickness channel. */
+void or_field_filter(const float *field2, uint32_t w, uint32_t h, float ex, float ey, float *out4);
+
 #ifdef __cplusplus
 }
 #endif

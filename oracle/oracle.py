@@ -100,6 +100,8 @@ def lib():
             "or_sim_tracers": (None, [C.c_void_p, C.POINTER(OrStep)]),
             "or_sim_advect": (None, [C.c_void_p, C.POINTER(OrStep)]),
             "or_sim_field": (None, [C.c_void_p, C.c_int, C.c_void_p]),
+            "or_field_splat": (None, [C.c_void_p] * 4 + [U, f32p, U, U, U, F, f32p]),
+            "or_field_filter": (None, [f32p, U, U, F, F, f32p]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -265,3 +267,22 @@ class Sim:
 
 def set_threads(n):
     lib().or_sim_set_threads(n)
+
+
+def field_splat(pos4, vel4, pvel4, density, geom, w, h, lens, keep, field2=None):
+    """The body splat with the decay draw over the given resting state;
+    returns the new field [h][w][2] (starting from `field2` or zeros)."""
+    pos4, vel4, pvel4 = f32(pos4), f32(vel4), f32(pvel4)
+    density = f32(density)
+    out = np.zeros((h, w, 2), np.float32) if field2 is None else f32(field2).copy()
+    lib().or_field_splat(_ptr(pos4), _ptr(vel4), _ptr(pvel4), _ptr(density), len(pos4),
+                         f32(geom), w, h, lens, keep, out)
+    return out
+
+
+def field_filter(field2, ex, ey):
+    h, w = field2.shape[:2]
+    out = np.zeros((h, w, 4), np.float32)
+    lib().or_field_filter(f32(field2), w, h, ex, ey, out)
+    return out
+
