@@ -188,14 +188,22 @@ int32_t batch_graph_tolerance(FluidBatch *s, cudaGraphExec_t *out) {
     cudaError_t e = grid_build_enqueue(st, s->b.pos, s->n, GridGeom{}, s->b.keys, s->b.starts, s->b.perm,
                                        s->gw, true, s->ring, s->cur, s->solve, kBatchRing, &bk);
     const Geo geo = s->geo();
+    // forces_eval after every divergence apply, forming the prediction that
+    // decides the loop (as the one-box tolerance substep)
+    const bool fused = c.max_iters >= 1;
+    SimBufs bd = s->b;
+    if (fused) {
+        bd.kd = s->b.kd2;
+        bd.wpk = s->b.wpk2;
+    }
     if (e == cudaSuccess) {
         launch_gather(st, s->b, s->n);
-        launch_density_div(st, geo, s->b, 0);
+        launch_density_div(st, geo, bd, 0);
         launch_tol_finish(st, geo, 0, 1, c.div_tol, c.max_iters, hdiv);
         rc = host_add_while(st, g, hdiv, &bdiv);
     }
     if (e == cudaSuccess && rc == FLUID_OK) {
-        launch_forces_eval(st, geo, s->b);
+        if (!fused) launch_forces_eval(st, geo, s->b);
         launch_forces_apply(st, geo, s->b);
         launch_den_kappa(st, geo, s->b, 0, kGateNone);
         launch_tol_finish(st, geo, 1, 1, c.den_tol, c.max_iters, hden);
@@ -212,8 +220,9 @@ int32_t batch_graph_tolerance(FluidBatch *s, cudaGraphExec_t *out) {
                                                 cudaGetErrorString(e != cudaSuccess ? e : e2));
     }
     BK(cudaStreamBeginCaptureToGraph(s->side, bdiv, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    launch_apply(s->side, geo, s->b, false, kGateDiv);
-    launch_div_kappa(s->side, geo, s->b, 0, kGateDiv);
+    launch_apply(s->side, geo, bd, false, kGateDiv);
+    if (fused) launch_forces_div(s->side, geo, s->b, 0, kGateDiv);
+    else launch_div_kappa(s->side, geo, s->b, 0, kGateDiv);
     launch_tol_finish(s->side, geo, 0, 0, c.div_tol, c.max_iters, hdiv);
     BK(cudaStreamEndCapture(s->side, &bdiv));
     BK(cudaStreamBeginCaptureToGraph(s->side, bden, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -330,6 +339,8 @@ int32_t batch_create_into(FluidBatch *s, const FluidSimConfig *boxes, uint32_t n
     BK(s->alloc(&b.alpha, n));
     BK(s->alloc(&b.kd, n));
     BK(s->alloc(&b.wpk, n));
+    BK(s->alloc(&b.kd2, n));
+    BK(s->alloc(&b.wpk2, n));
     BK(s->alloc(&b.pressure, n));
     BK(s->alloc(&b.pinc, n));
     BK(s->alloc(&b.rho_near, n));

@@ -401,14 +401,23 @@ int32_t capture_tolerance(FluidSim *s, cudaGraphExec_t *out) {
         e = grid_build_enqueue(st, s->b.pos, s->n, geom_of(s->P), s->b.keys, s->b.starts, s->b.perm, s->gw,
                                true, s->ring, s->cur, s->solve, kRing);
     const Geo geo = s->geo();
+    // With at least one divergence apply, forces_eval runs after every one
+    // and also forms the divergence prediction that decides whether the
+    // loop goes on (its kappa in kd2 / wpk2, which the loop's applies read).
+    const bool fused = c.max_iters >= 1;
+    SimBufs bd = s->b;
+    if (fused) {
+        bd.kd = s->b.kd2;
+        bd.wpk = s->b.wpk2;
+    }
     if (e == cudaSuccess) {
         launch_gather(st, s->b, s->n);
-        launch_density_div(st, geo, s->b, 0);
+        launch_density_div(st, geo, bd, 0);
         launch_tol_finish(st, geo, 0, 1, c.div_tol, c.max_iters, hdiv);
         rc = add_while(st, g, hdiv, &bdiv);
     }
     if (e == cudaSuccess && rc == FLUID_OK) {
-        launch_forces_eval(st, geo, s->b);
+        if (!fused) launch_forces_eval(st, geo, s->b);
         launch_forces_apply(st, geo, s->b);
         launch_den_kappa(st, geo, s->b, 0, kGateNone);
         launch_tol_finish(st, geo, 1, 1, c.den_tol, c.max_iters, hden);
@@ -426,8 +435,9 @@ int32_t capture_tolerance(FluidSim *s, cudaGraphExec_t *out) {
     }
     // loop bodies
     CK(cudaStreamBeginCaptureToGraph(s->side, bdiv, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    launch_apply(s->side, geo, s->b, false, kGateDiv);
-    launch_div_kappa(s->side, geo, s->b, 0, kGateDiv);
+    launch_apply(s->side, geo, bd, false, kGateDiv);
+    if (fused) launch_forces_div(s->side, geo, s->b, 0, kGateDiv);
+    else launch_div_kappa(s->side, geo, s->b, 0, kGateDiv);
     launch_tol_finish(s->side, geo, 0, 0, c.div_tol, c.max_iters, hdiv);
     CK(cudaStreamEndCapture(s->side, &bdiv));
     CK(cudaStreamBeginCaptureToGraph(s->side, bden, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -653,6 +663,8 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(s->alloc(&b.alpha, n));
     CK(s->alloc(&b.kd, n));
     CK(s->alloc(&b.wpk, n));
+    CK(s->alloc(&b.kd2, n));
+    CK(s->alloc(&b.wpk2, n));
     CK(s->alloc(&b.pressure, n));
     CK(s->alloc(&b.pinc, n));
     CK(s->alloc(&b.rho_near, n));

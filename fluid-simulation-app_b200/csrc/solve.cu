@@ -624,12 +624,22 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int a
 }
 
 // ---- forces_eval (sim_solve.wgsl:524-592) ---------------------------------
-template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_eval(Geo g, SimBufs b) {
+// With kDiv, the same walk also forms the divergence prediction of
+// k_div_kappa (the same pair terms, in the same order, so the same sums):
+// its kappa goes to kd2 / wpk2 and its residual term to acc_div[slot], and
+// boxes whose divergence loop has stopped (gate) are skipped. The tolerance
+// schedule runs this after each divergence apply, so the prediction that
+// only decides whether the loop stops costs no sweep of its own.
+template <bool kB, bool kDiv>
+__device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b, int slot, int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const DevParams P = params_of<kB>(g, box_index<kB>(g, i));
+    const bool live = i < n;
+    if (!kDiv && !live) return;
+    const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
+    unsigned long long term = 0;
+    if (live && !(kDiv && gated_out<kB>(g, bi, gate))) {
+    const DevParams P = params_of<kB>(g, bi);
     const float coh_c = 2.0f * P.h;
     const float c3 = coh_c * coh_c * coh_c;
     const float coh_k = 32.0f / (3.14159265f * c3 * c3 * c3);
@@ -650,7 +660,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_eval(Geo g, SimBufs b)
     const uint32_t cnt = __ldg(&b.nbr_n[i]);
     F3 visc = f3(0.f, 0.f, 0.f), blend = f3(0.f, 0.f, 0.f), near = f3(0.f, 0.f, 0.f),
        tension = f3(0.f, 0.f, 0.f);
-    float heat = 0.0f;
+    float heat = 0.0f, drho = 0.0f;
     auto load = [&](uint32_t j) {
         return Nbr5{__ldg(&b.wpos[j]), __ldg(&b.wvel[j]), __ldg(&b.density[j]), __ldg(&b.wtemp[j]),
                     __ldg(&b.rho_near[j])};
@@ -665,6 +675,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_eval(Geo g, SimBufs b)
         const float f = dot(x, e) / (r2 + 0.01f * P.h * P.h);
         const float pair = P.mass / (rho_i * rho_j) * f;
         const F3 dv = vel - xyz(q.v);
+        if (kDiv) drho += dot(dv, e);
         const float wn = fmaxf(1.0f - r * P.inv_h, 0.0f);
         near = near + ((near_i + q.near) * wn * wn) * (x / fmaxf(r, 1e-5f));
         visc = visc + (visc_k * pair) * dv;
@@ -683,6 +694,26 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_eval(Geo g, SimBufs b)
     b.kd[i] = kdv;
     b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
     b.pressure[i] = half;
+    if (kDiv) {  // k_div_kappa's prediction
+        const float dt = g.st[bi].s.dt;
+        drho = P.mass * drho;
+        drho += dot(vel, xyz(__ldg(&b.wgrad[i])));
+        const float kdd = fmaxf(drho, 0.0f) * __ldg(&b.alpha[i]) / fmaxf(dt, 1e-9f) / rho_i;
+        b.kd2[i] = kdd;
+        b.wpk2[i] = make_float4(pos.x, pos.y, pos.z, kdd);
+        term = fixed_term((double)fmaxf(drho, 0.0f) * (double)dt / (double)P.rho0);
+    }
+    }
+    if (kDiv) add_term<kB>(&g.solve[bi].acc_div[slot], term);
+}
+
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
+    forces_eval_body<kB, false>(g, b, slot, gate);
+}
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
+    forces_eval_body<kB, true>(g, b, slot, gate);
 }
 
 // fingers (sim_solve.wgsl:103-127)
@@ -1124,7 +1155,10 @@ void launch_apply(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_press
     FCU_SWEEP(k_apply, kTuneApply, kSolveThreads, g, b, add_pressure ? 1 : 0, gate);
 }
 void launch_forces_eval(cudaStream_t s, const Geo &g, const SimBufs &b) {
-    FCU_SWEEP(k_forces_eval, kTuneForcesEval, kSolveThreads, g, b);
+    FCU_SWEEP(k_forces_plain, kTuneForcesEval, kSolveThreads, g, b, 0, kGateNone);
+}
+void launch_forces_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
+    FCU_SWEEP(k_forces_fused, kTuneForcesEval, kSolveThreads, g, b, slot, gate);
 }
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b) {
     FCU_SWEEP(k_forces_apply, kTuneForcesApply, kSolveThreads, g, b);

@@ -23,6 +23,10 @@ struct SimBufs {
     float *density, *alpha, *kd, *pressure, *pinc, *rho_near;
     float4 *accel, *xsph, *wgrad;
     float4 *wpk;  // position and kd of the last prediction: apply's one record per neighbour
+    // the divergence loop's own kd and (position, kd) in the tolerance
+    // schedule, where forces_eval also forms the divergence prediction
+    float *kd2;
+    float4 *wpk2;
     // Neighbour list, slot-major (entry k of particle i at k * n + i): the
     // neighbour's slot and the bits of its kernel-gradient scale dw / r,
     // so a sweep forms the gradient (dw / r) * (x_i - x_j) without the
@@ -83,6 +87,10 @@ void launch_density_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot
 void launch_div_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate);
 void launch_apply(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int gate);
 void launch_forces_eval(cudaStream_t s, const Geo &g, const SimBufs &b);
+// forces_eval that also forms the divergence prediction (kappa into kd2 /
+// wpk2, residual term into acc_div[slot]), skipping boxes whose divergence
+// loop has stopped.
+void launch_forces_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate);
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b);
 void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate);
 // div_slot >= 0: record each box's residuals from those accumulator slots
