@@ -29,6 +29,18 @@
 #ifndef FCU_B_N5
 #define FCU_B_N5 1
 #endif
+// Minimum resident blocks per SM that density_div (one box, at 128 threads
+// a block; scaled for other block sizes) and the kappa sweeps are
+// compiled for (0: none), and density_div's hits staged per round.
+#ifndef FCU_MINB_DD
+#define FCU_MINB_DD 7
+#endif
+#ifndef FCU_MINB_KAPPA
+#define FCU_MINB_KAPPA 0
+#endif
+#ifndef FCU_STAGE
+#define FCU_STAGE 32
+#endif
 #ifndef FCU_MINB
 #define FCU_MINB 0
 #endif
@@ -397,7 +409,7 @@ __device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d
 // the stores of a round coalesce. The neighbours are summed in the same
 // order as the plain loop, so every sum is the same sum. A stencil row wider
 // than a code's 4,096-slot offset falls back to the plain loop.
-constexpr int kStage = 32;
+constexpr int kStage = FCU_STAGE;
 constexpr uint32_t kRowSpan = 4096;
 
 // The plain loop over every candidate, each hit summed and the first `cap`
@@ -424,7 +436,7 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
 }
 
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB) k_density_div(Geo g, SimBufs b, int slot) {
+__global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_density_div(Geo g, SimBufs b, int slot) {
     __shared__ uint16_t s_hit[kStage][TPB];
     __shared__ uint32_t s_beg[9][TPB];
     __shared__ uint32_t s_end[9][TPB];
@@ -558,7 +570,7 @@ __device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
 // density_div's divergence sums again over the list, with this
 // iteration's velocities.
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB) k_div_kappa(Geo g, SimBufs b, int slot,
+__global__ void __launch_bounds__(TPB, FCU_MINB_KAPPA) k_div_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -767,7 +779,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_apply(Geo g, SimBufs b
 
 // ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB) k_den_kappa(Geo g, SimBufs b, int slot,
+__global__ void __launch_bounds__(TPB, FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
