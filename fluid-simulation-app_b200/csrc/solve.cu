@@ -41,6 +41,14 @@
 #ifndef FCU_STAGE
 #define FCU_STAGE 32
 #endif
+// Candidates density_div loads before testing any (a round may then stage
+// up to FCU_STAGE + FCU_DD_CHUNK - 1 hits).
+#ifndef FCU_DD_P2
+#define FCU_DD_P2 2
+#endif
+#ifndef FCU_DD_CHUNK
+#define FCU_DD_CHUNK 4
+#endif
 #ifndef FCU_MINB
 #define FCU_MINB 0
 #endif
@@ -227,6 +235,15 @@ __device__ __forceinline__ F3 pair_grad(float scale, F3 pos, float4 pj) {
 #ifndef FCU_PREFETCH
 #define FCU_PREFETCH 1
 #endif
+// FCU_L2PF > 0: each batch also asks L2 for the list rows FCU_L2PF batches
+// past the next one (no registers held), so the entries' DRAM round trip
+// starts earlier.
+#ifndef FCU_L2PF
+#define FCU_L2PF 1
+#endif
+__device__ __forceinline__ void prefetch_l2(const void *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
 __device__ __forceinline__ uint2 list_ld(const uint2 *p) {
 #if FCU_LIST_CS
     return __ldcs(p);
@@ -250,6 +267,13 @@ __device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, 
 #pragma unroll
         for (int u = 0; u < B; ++u)
             en[u] = (k + B + u < cnt) ? list_ld(&nbr[(size_t)(k + B + u) * n + i]) : make_uint2(i, 0u);
+#if FCU_L2PF
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const uint32_t kf = k + B * (1 + FCU_L2PF) + u;
+            if (kf < cnt) prefetch_l2(&nbr[(size_t)kf * n + i]);
+        }
+#endif
 #pragma unroll
         for (int u = 0; u < B; ++u)
             if (k + u < cnt) use(__uint_as_float(e[u].y), v[u]);
@@ -410,6 +434,7 @@ __device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d
 // order as the plain loop, so every sum is the same sum. A stencil row wider
 // than a code's 4,096-slot offset falls back to the plain loop.
 constexpr int kStage = FCU_STAGE;
+constexpr int kP2 = FCU_DD_P2;
 constexpr uint32_t kRowSpan = 4096;
 
 // The plain loop over every candidate, each hit summed and the first `cap`
@@ -437,7 +462,7 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
 
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_density_div(Geo g, SimBufs b, int slot) {
-    __shared__ uint16_t s_hit[kStage][TPB];
+    __shared__ uint16_t s_hit[kStage + FCU_DD_CHUNK - 1][TPB];
     __shared__ uint32_t s_beg[9][TPB];
     __shared__ uint32_t s_end[9][TPB];
     const uint32_t n = g.n;
@@ -486,6 +511,26 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
                         e = s_end[r][tid];
                         continue;
                     }
+#if FCU_DD_CHUNK > 1
+                    {
+                        float4 pc[FCU_DD_CHUNK];
+#pragma unroll
+                        for (int u = 0; u < FCU_DD_CHUNK; ++u) {
+                            const uint32_t ku = k + u;
+                            pc[u] = __ldg(&b.wpos[ku < e ? ku : i]);
+                        }
+#pragma unroll
+                        for (int u = 0; u < FCU_DD_CHUNK; ++u) {
+                            const uint32_t ku = k + u;
+                            const F3 x = pos - xyz(pc[u]);
+                            if (ku < e && ku != i && dot(x, x) < P.support_sq) {
+                                s_hit[staged][tid] = (uint16_t)((r << 12) | (ku - rs));
+                                ++staged;
+                            }
+                        }
+                        k = (e - k > (uint32_t)FCU_DD_CHUNK) ? k + FCU_DD_CHUNK : e;
+                    }
+#else
                     if (k != i) {
                         const F3 x = pos - xyz(__ldg(&b.wpos[k]));
                         if (dot(x, x) < P.support_sq) {
@@ -494,24 +539,25 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
                         }
                     }
                     ++k;
+#endif
                 }
-                // phase 2: the staged hits, in order, two loads in flight
-                for (uint32_t h = 0; h < staged; h += 2) {
-                    uint32_t j[2];
+                // phase 2: the staged hits, in order, kP2 loads in flight
+                for (uint32_t h = 0; h < staged; h += kP2) {
+                    uint32_t j[kP2];
 #pragma unroll
-                    for (int u = 0; u < 2; ++u) {
+                    for (int u = 0; u < kP2; ++u) {
                         const bool ok = h + u < staged;
                         const uint32_t code = ok ? (uint32_t)s_hit[h + u][tid] : 0u;
                         j[u] = ok ? s_beg[code >> 12][tid] + (code & (kRowSpan - 1u)) : i;
                     }
-                    float4 pj[2], vj[2];
+                    float4 pj[kP2], vj[kP2];
 #pragma unroll
-                    for (int u = 0; u < 2; ++u) {
+                    for (int u = 0; u < kP2; ++u) {
                         pj[u] = __ldg(&b.wpos[j[u]]);
                         vj[u] = __ldg(&b.wvel[j[u]]);
                     }
 #pragma unroll
-                    for (int u = 0; u < 2; ++u) {
+                    for (int u = 0; u < kP2; ++u) {
                         if (h + u < staged) {
                             const F3 x = pos - xyz(pj[u]);
                             const float gs = density_pair(P, d, pos, vel, x, dot(x, x), vj[u]);
