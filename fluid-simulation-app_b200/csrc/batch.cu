@@ -297,7 +297,7 @@ int32_t batch_create_into(FluidBatch *s, const FluidSimConfig *boxes, uint32_t n
         s->cell_base.push_back((uint32_t)cells64);
         n64 += cnt;
         cells64 += c;
-        if (n64 > 0x7fffffffull) return report_error(FLUID_ERR_ARG, "a batch holds at most 2^31-1 particles");
+        if (n64 > 0x0fffffffull) return report_error(FLUID_ERR_ARG, "a batch holds at most 2^28-1 particles");
         if (cells64 >= 0xffffffffull) return report_error(FLUID_ERR_ARG, "the batch's grids have too many cells");
         pos.insert(pos.end(), p.begin(), p.end());
         temp.insert(temp.end(), cnt, boxes[bx].temperature);

@@ -632,7 +632,8 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     else if (cfg->seeding == FLUID_SEED_BLOCK) seed_block(*cfg, pos);
     else pos.assign(4ull * cfg->count, 0.0f);
     const uint64_t n64 = pos.size() / 4;
-    if (n64 == 0 || n64 > 0x7fffffffull) return fail(FLUID_ERR_ARG, "particle count must be in 1..2^31-1");
+    // a neighbour list entry holds the slot in 28 bits
+    if (n64 == 0 || n64 > 0x0fffffffull) return fail(FLUID_ERR_ARG, "particle count must be in 1..2^28-1");
     s->n = (uint32_t)n64;
     derive_params(*cfg, s->n, s->P);
     const uint64_t cells64 = (uint64_t)s->P.dims[0] * s->P.dims[1] * s->P.dims[2];

@@ -170,7 +170,8 @@ void fluid_sim_default_config(FluidSimConfig *cfg);
 
 /* Replaces fluid_renderer_create (fluid_ffi.h:74-83; lib.rs:72-109) for the
  * sim alone: builds the particles, the grid and every device buffer, and
- * captures the substep as a CUDA graph. Null on failure, reason in
+ * captures the substep as a CUDA graph. At most 2^28 - 1 particles (a
+ * batch too, over all its boxes). Null on failure, reason in
  * fluid_last_error() and on stderr. */
 FluidSim *fluid_sim_create(const FluidSimConfig *cfg);
 
