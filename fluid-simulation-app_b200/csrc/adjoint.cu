@@ -368,7 +368,8 @@ __global__ void __launch_bounds__(256) k_m_pos4(const V3<T> *__restrict__ x, flo
 }
 
 // Neighbour list of every particle (stencil order, grid order inside a
-// cell), density, near density, alpha and the wall gradient. With `perm`
+// cell) with each pair's gradient scale gs (into gsl when given), density,
+// near density, alpha and the wall gradient. With `perm`
 // null the particles are in the grid's cell order (slot k is particle k);
 // otherwise slot k holds particle perm[k].
 template <class T>
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
                                                            const float4 *__restrict__ pos4,
                                                            const uint32_t *__restrict__ starts,
                                                            const uint32_t *__restrict__ perm, uint32_t *nbr,
-                                                           uint32_t *nbr_n, T *rho, T *rhon, T *alpha,
+                                                           T *gsl, uint32_t *nbr_n, T *rho, T *rhon, T *alpha,
                                                            V3<T> *wg, uint32_t *over) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -410,7 +411,10 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
                 const V3<T> gw = R.gs * xij;
                 gsum = gsum + gw;
                 gsq += dot(gw, gw);
-                if (cnt < kModelCap) nbr[(size_t)cnt * n + i] = j;
+                if (cnt < kModelCap) {
+                    nbr[(size_t)cnt * n + i] = j;
+                    if (gsl) gsl[(size_t)cnt * n + i] = R.gs;
+                }
                 cnt++;
             }
         }
@@ -446,19 +450,100 @@ __global__ void __launch_bounds__(256) k_m_gather(uint32_t n, const uint32_t *__
     perm_out[k] = j;
 }
 
+// Walks particle i's list in order, kMB entries at a time: the entries and
+// their gradient scales, then the neighbours' records (load(j)), and only
+// then use(gs, record) for each, so a batch's loads overlap. Same order as
+// a plain loop, so the same sums.
+constexpr int kMB = 4;
+constexpr int kRB = 2;  // the reverse sweeps with wide records
+template <class T, class R, class Load, class Use>
+DEV void mwalk(const uint32_t *__restrict__ nbr, const T *__restrict__ gsl, uint32_t n, uint32_t i,
+               uint32_t cnt, Load load, Use use) {
+    for (uint32_t k = 0; k < cnt; k += kMB) {
+        uint32_t j[kMB];
+        T g[kMB];
+#pragma unroll
+        for (int u = 0; u < kMB; ++u) {
+            const bool ok = k + u < cnt;
+            j[u] = ok ? nbr[(size_t)(k + u) * n + i] : i;
+            g[u] = ok ? gsl[(size_t)(k + u) * n + i] : T(0);
+        }
+        R r[kMB];
+#pragma unroll
+        for (int u = 0; u < kMB; ++u) r[u] = load(j[u]);
+#pragma unroll
+        for (int u = 0; u < kMB; ++u)
+            if (k + u < cnt) use(g[u], r[u]);
+    }
+}
+template <class T> struct XV {
+    V3<T> x, v;
+};
+template <class T> struct XK {
+    V3<T> x;
+    T kd;
+};
+
+// mwalk for the reverse sweeps, which keep no gradient scales: kB entries,
+// then their records, then use(j, record) for each, in list order.
+template <int kB, class R, class Load, class Use>
+DEV void rwalk(const uint32_t *__restrict__ nbr, uint32_t n, uint32_t i, uint32_t cnt, Load load, Use use) {
+    for (uint32_t k = 0; k < cnt; k += kB) {
+        uint32_t j[kB];
+#pragma unroll
+        for (int u = 0; u < kB; ++u) j[u] = k + u < cnt ? nbr[(size_t)(k + u) * n + i] : i;
+        R r[kB];
+#pragma unroll
+        for (int u = 0; u < kB; ++u) r[u] = load(j[u]);
+#pragma unroll
+        for (int u = 0; u < kB; ++u)
+            if (k + u < cnt) use(j[u], r[u]);
+    }
+}
+template <class T> struct XVK {
+    V3<T> x, v;
+    T k;
+};
+
 // d_i = m sum (v_i - v_j).grad W_ij + v_i.wg_i
 template <class T>
 DEV T div_of(const MP<T> &p, uint32_t n, uint32_t i, const V3<T> *__restrict__ x, const V3<T> *__restrict__ v,
-             const uint32_t *__restrict__ nbr, uint32_t cnt, V3<T> wgi) {
+             const uint32_t *__restrict__ nbr, const T *__restrict__ gsl, uint32_t cnt, V3<T> wgi) {
     const V3<T> xi = x[i], vi = v[i];
     T d = T(0);
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        d += dot(vi - v[j], R.gs * xij);
-    }
+    mwalk<T, XV<T>>(
+        nbr, gsl, n, i, cnt, [&](uint32_t j) { return XV<T>{x[j], v[j]}; },
+        [&](T gs, const XV<T> &q) { d += dot(vi - q.v, gs * (xi - q.x)); });
     return p.m * d + dot(vi, wgi);
+}
+
+// div_of with each pair's gradient scale recomputed (the reverse sweeps,
+// which keep no scales): the same values, so the same sum.
+template <class T>
+DEV T div_of_radial(const MP<T> &p, uint32_t n, uint32_t i, const V3<T> *__restrict__ x,
+                    const V3<T> *__restrict__ v, const uint32_t *__restrict__ nbr, uint32_t cnt, V3<T> wgi) {
+    const V3<T> xi = x[i], vi = v[i];
+    T d = T(0);
+    rwalk<kMB, XV<T>>(
+        nbr, n, i, cnt, [&](uint32_t j) { return XV<T>{x[j], v[j]}; },
+        [&](uint32_t, const XV<T> &q) {
+            const V3<T> xij = xi - q.x;
+            const Radial<T> R = radial(p, dot(xij, xij));
+            d += dot(vi - q.v, R.gs * xij);
+        });
+    return p.m * d + dot(vi, wgi);
+}
+
+// sum (kd_i + kd_j) grad W_ij
+template <class T>
+DEV V3<T> kappa_of(uint32_t n, uint32_t i, V3<T> xi, T kdi, const V3<T> *__restrict__ x,
+                   const T *__restrict__ kd, const uint32_t *__restrict__ nbr, const T *__restrict__ gsl,
+                   uint32_t cnt) {
+    V3<T> s = zero3<T>();
+    mwalk<T, XK<T>>(
+        nbr, gsl, n, i, cnt, [&](uint32_t j) { return XK<T>{x[j], kd[j]}; },
+        [&](T gs, const XK<T> &q) { s = s + (kdi + q.kd) * (gs * (xi - q.x)); });
+    return s;
 }
 
 // Divergence (den = 0) or density (den = 1) prediction; the residual term
@@ -466,14 +551,14 @@ DEV T div_of(const MP<T> &p, uint32_t n, uint32_t i, const V3<T> *__restrict__ x
 template <class T>
 __global__ void __launch_bounds__(kAdjThreads) k_m_kappa(MP<T> p, uint32_t n, int den, T dt,
                                                          const V3<T> *__restrict__ x, const V3<T> *__restrict__ v,
-                                                         const uint32_t *__restrict__ nbr,
+                                                         const uint32_t *__restrict__ nbr, const T *__restrict__ gsl,
                                                          const uint32_t *__restrict__ nbr_n, const T *__restrict__ rho,
                                                          const T *__restrict__ alpha, const V3<T> *__restrict__ wg,
                                                          T *kd, T *pinc, double *res) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double term = 0.0;
     if (i < n) {
-        const T d = div_of(p, n, i, x, v, nbr, nbr_n[i], wg[i]);
+        const T d = div_of(p, n, i, x, v, nbr, gsl, nbr_n[i], wg[i]);
         const T r = rho[i], a = alpha[i];
         if (!den) {
             const T dp = d > T(0) ? d : T(0);
@@ -500,7 +585,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_kappa(MP<T> p, uint32_t n, in
 template <class T>
 __global__ void __launch_bounds__(kAdjThreads) k_m_apply(MP<T> p, uint32_t n, T dt, const V3<T> *__restrict__ x,
                                                          const V3<T> *v_in, V3<T> *v_out,
-                                                         const uint32_t *__restrict__ nbr,
+                                                         const uint32_t *__restrict__ nbr, const T *__restrict__ gsl,
                                                          const uint32_t *__restrict__ nbr_n, const T *__restrict__ kd,
                                                          const V3<T> *__restrict__ wg, const T *__restrict__ pinc,
                                                          T *pressure) {
@@ -508,14 +593,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_apply(MP<T> p, uint32_t n, T 
     if (i >= n) return;
     const V3<T> xi = x[i];
     const T kdi = kd[i];
-    const uint32_t cnt = nbr_n[i];
-    V3<T> s = zero3<T>();
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        s = s + (kdi + kd[j]) * (R.gs * xij);
-    }
+    const V3<T> s = kappa_of(n, i, xi, kdi, x, kd, nbr, gsl, nbr_n[i]);
     const V3<T> dv = p.m * s + kdi * wg[i];
     v_out[i] = v_in[i] - dt * dv;
     if (pinc) pressure[i] += pinc[i];
@@ -576,20 +654,14 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_forces_apply(MP<T> p, uint32_
                                                                 V3<T> *v_out, const V3<T> *__restrict__ accel,
                                                                 const V3<T> *__restrict__ blend,
                                                                 const uint32_t *__restrict__ nbr,
+                                                                const T *__restrict__ gsl,
                                                                 const uint32_t *__restrict__ nbr_n,
                                                                 const T *__restrict__ kd, const V3<T> *__restrict__ wg) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const V3<T> xi = x[i];
     const T kdi = kd[i];
-    const uint32_t cnt = nbr_n[i];
-    V3<T> s = zero3<T>();
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        s = s + (kdi + kd[j]) * (R.gs * xij);
-    }
+    const V3<T> s = kappa_of(n, i, xi, kdi, x, kd, nbr, gsl, nbr_n[i]);
     const V3<T> forced = v_in[i] + dt * (f + accel[i]) + c * blend[i];
     v_out[i] = forced - dt * (p.m * s + kdi * wg[i]);
 }
@@ -708,14 +780,15 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_apply(MP<T> p, uint32_t n, T 
     const uint32_t cnt = nbr_n[i];
     T s = T(0);
     V3<T> xs = zero3<T>();
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        const V3<T> dvb = vb - vbar[j];
-        s += dot(R.gs * xij, dvb);
-        xs = xs + (c * (kdi + kd[j])) * hess(R, xij, dvb);
-    }
+    rwalk<kMB, XVK<T>>(
+        nbr, n, i, cnt, [&](uint32_t j) { return XVK<T>{x[j], vbar[j], kd[j]}; },
+        [&](uint32_t, const XVK<T> &q) {
+            const V3<T> xij = xi - q.x;
+            const Radial<T> R = radial(p, dot(xij, xij));
+            const V3<T> dvb = vb - q.v;
+            s += dot(R.gs * xij, dvb);
+            xs = xs + (c * (kdi + q.k)) * hess(R, xij, dvb);
+        });
     const V3<T> wgi = wg[i];
     kdbar[i] = -dt * (p.m * s + dot(wgi, vb));
     const J3<T> J = wall_grad_jac(p, xi);
@@ -737,7 +810,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_kappa_a(MP<T> p, uint32_t n, 
                                                            T *alphabar) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const T d = div_of(p, n, i, x, v, nbr, nbr_n[i], wg[i]);
+    const T d = div_of_radial(p, n, i, x, v, nbr, nbr_n[i], wg[i]);
     const T r = rho[i], a = alpha[i], kb = kdbar[i];
     T db = T(0), rb = T(0), ab = T(0);
     if (!den) {
@@ -780,15 +853,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_kappa_b(MP<T> p, uint32_t n, 
     const T di = dbar[i];
     const uint32_t cnt = nbr_n[i];
     V3<T> vs = zero3<T>(), xs = zero3<T>();
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const T c = p.m * (di + dbar[j]);
-        if (c == T(0)) continue;
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        vs = vs + (c * R.gs) * xij;
-        xs = xs + c * hess(R, xij, vi - v[j]);
-    }
+    rwalk<kMB, XVK<T>>(
+        nbr, n, i, cnt, [&](uint32_t j) { return XVK<T>{x[j], v[j], dbar[j]}; },
+        [&](uint32_t, const XVK<T> &q) {
+            const T c = p.m * (di + q.k);
+            if (c == T(0)) return;
+            const V3<T> xij = xi - q.x;
+            const Radial<T> R = radial(p, dot(xij, xij));
+            vs = vs + (c * R.gs) * xij;
+            xs = xs + c * hess(R, xij, vi - q.v);
+        });
     vbar[i] = vbar[i] + vs + di * wg[i];
     if (di != T(0)) {
         const J3<T> J = wall_grad_jac(p, xi);
@@ -824,14 +898,15 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_
         const uint32_t cnt = nbr_n[i];
         T s = T(0);
         V3<T> xs = zero3<T>();
-        for (uint32_t k = 0; k < cnt; ++k) {
-            const uint32_t j = nbr[(size_t)k * n + i];
-            const V3<T> xij = xi - x[j];
-            const Radial<T> R = radial(p, dot(xij, xij));
-            const V3<T> dvb = vb - vbar[j];
-            s += dot(R.gs * xij, dvb);
-            xs = xs + (cc * (kdi + kd[j])) * hess(R, xij, dvb);
-        }
+        rwalk<kMB, XVK<T>>(
+            nbr, n, i, cnt, [&](uint32_t j) { return XVK<T>{x[j], vbar[j], kd[j]}; },
+            [&](uint32_t, const XVK<T> &q) {
+                const V3<T> xij = xi - q.x;
+                const Radial<T> R = radial(p, dot(xij, xij));
+                const V3<T> dvb = vb - q.v;
+                s += dot(R.gs * xij, dvb);
+                xs = xs + (cc * (kdi + q.k)) * hess(R, xij, dvb);
+            });
         const V3<T> wgi = wg[i];
         kdbar[i] = -dt * (p.m * s + dot(wgi, vb));
         const J3<T> J = wall_grad_jac(p, xi);
@@ -962,20 +1037,24 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_eval(MP<T> p, uint32_t
     T nb_i = T(0);
     V3<T> xs = zero3<T>(), vs = zero3<T>();
     const uint32_t cnt = nbr_n[i];
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const T r2 = dot(xij, xij);
-        const Radial<T> R = radial(p, r2);
-        const T rho_j = rho[j], near_j = rhon[j];
-        const V3<T> dv = vi - v[j];
-        const PairBar<T> own = forces_pair_bar(p, xij, r2, R, dv, rho_i, rho_j, near_i, near_j, ab, bb);
-        const PairBar<T> oth = forces_pair_bar(p, -xij, r2, R, -dv, rho_j, rho_i, near_j, near_i, abar[j], bbar[j]);
-        xs = xs + own.gx - oth.gx;
-        vs = vs + own.gdv - oth.gdv;
-        rb_i += own.rb_a + oth.rb_b;
-        nb_i += own.nb + oth.nb;
-    }
+    struct Rec {
+        V3<T> x, v, ab, bb;
+        T rho, near;
+    };
+    rwalk<kRB, Rec>(
+        nbr, n, i, cnt, [&](uint32_t j) { return Rec{x[j], v[j], abar[j], bbar[j], rho[j], rhon[j]}; },
+        [&](uint32_t, const Rec &q) {
+            const V3<T> xij = xi - q.x;
+            const T r2 = dot(xij, xij);
+            const Radial<T> R = radial(p, r2);
+            const V3<T> dv = vi - q.v;
+            const PairBar<T> own = forces_pair_bar(p, xij, r2, R, dv, rho_i, q.rho, near_i, q.near, ab, bb);
+            const PairBar<T> oth = forces_pair_bar(p, -xij, r2, R, -dv, q.rho, rho_i, q.near, near_i, q.ab, q.bb);
+            xs = xs + own.gx - oth.gx;
+            vs = vs + own.gdv - oth.gdv;
+            rb_i += own.rb_a + oth.rb_b;
+            nb_i += own.nb + oth.nb;
+        });
     const J3<T> Ja = wall_adh_jac(p, xi);
     xs = xs + (p.beta * p.rho0) * jt_mul(Ja, ab);
     xbar[i] = xbar[i] + xs;
@@ -1000,14 +1079,15 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density_a(MP<T> p, uint32_t n
     const uint32_t cnt = nbr_n[i];
     V3<T> gsum = zero3<T>();
     T gsq = T(0);
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        const V3<T> gw = R.gs * xij;
-        gsum = gsum + gw;
-        gsq += dot(gw, gw);
-    }
+    rwalk<kMB, V3<T>>(
+        nbr, n, i, cnt, [&](uint32_t j) { return x[j]; },
+        [&](uint32_t, const V3<T> &xj) {
+            const V3<T> xij = xi - xj;
+            const Radial<T> R = radial(p, dot(xij, xij));
+            const V3<T> gw = R.gs * xij;
+            gsum = gsum + gw;
+            gsq += dot(gw, gw);
+        });
     const V3<T> G = p.m * gsum + wall_grad(p, xi);
     const T den = dot(G, G) + p.m * p.m * gsq;
     const T r = rho[i];
@@ -1060,13 +1140,17 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density_b(MP<T> p, uint32_t n
     const V3<T> Gb = gbar[i];
     const uint32_t cnt = nbr_n[i];
     V3<T> xs = zero3<T>();
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
-        const Radial<T> R = radial(p, dot(xij, xij));
-        xs = xs + density_pair_bar(p, xij, R, rb, Gb, Sb, nb) -
-             density_pair_bar(p, -xij, R, rbt[j], gbar[j], sbar[j], rhonbar[j]);
-    }
+    struct Rec {
+        V3<T> x, gb;
+        T rb, sb, nb;
+    };
+    rwalk<kRB, Rec>(
+        nbr, n, i, cnt, [&](uint32_t j) { return Rec{x[j], gbar[j], rbt[j], sbar[j], rhonbar[j]}; },
+        [&](uint32_t, const Rec &q) {
+            const V3<T> xij = xi - q.x;
+            const Radial<T> R = radial(p, dot(xij, xij));
+            xs = xs + density_pair_bar(p, xij, R, rb, Gb, Sb, nb) - density_pair_bar(p, -xij, R, q.rb, q.gb, q.sb, q.nb);
+        });
     const J3<T> J = wall_grad_jac(p, xi);
     xs = xs + jt_mul(J, Gb) + (rb * p.rho0) * fill_grad(p, xi);
     xbar[i] = xbar[i] + xs;
@@ -1167,6 +1251,7 @@ struct AdjImpl : AdjBase {
     uint32_t seg_div_cap = 0, seg_den_cap = 0;
     Tape<T> fin;  // the final density pass of the loss
     T *kd = nullptr, *pinc = nullptr, *pressure = nullptr;
+    T *gsl = nullptr;  // the substep's gradient scales beside its list (forward sweeps only)
     double *acc = nullptr;  // residual (1), loss sums (4)
     // controls of the last forward
     std::vector<double> forces;
@@ -1277,6 +1362,7 @@ struct AdjImpl : AdjBase {
         rc = alloc_tape(fin, 0, 0, false);
         if (rc != FLUID_OK) return rc;
         AK(alloc(&kd, N));
+        AK(alloc(&gsl, N * kModelCap));
         AK(alloc(&pinc, N));
         AK(alloc(&pressure, N));
         AK(alloc(&acc, 8));
@@ -1338,7 +1424,7 @@ struct AdjImpl : AdjBase {
         const int32_t rc = grid(xs);
         if (rc != FLUID_OK) return rc;
         k_m_density<T><<<nblk(n, kAdjThreads), kAdjThreads, 0, stream>>>(
-            mp, n, xs, pos4, starts, perm, t.nbr, t.nbr_n, t.rho, t.rhon, t.alpha, t.wg, over);
+            mp, n, xs, pos4, starts, perm, t.nbr, nullptr, t.nbr_n, t.rho, t.rhon, t.alpha, t.wg, over);
         AK(cudaGetLastError());
         return FLUID_OK;
     }
@@ -1362,13 +1448,13 @@ struct AdjImpl : AdjBase {
         k_m_gather<T><<<nblk(n, 256), 256, 0, stream>>>(n, perm, x, v, pp, id, t.x, t.vdiv[0], t.pp, id2, t.perm);
         std::swap(id, id2);
         const uint32_t B = nblk(n, kAdjThreads);
-        k_m_density<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, pos4, starts, nullptr, t.nbr, t.nbr_n, t.rho,
-                                                      t.rhon, t.alpha, t.wg, over);
+        k_m_density<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, pos4, starts, nullptr, t.nbr, gsl, t.nbr_n,
+                                                      t.rho, t.rhon, t.alpha, t.wg, over);
         // divergence loop
         uint32_t nd = decide ? 0u : div_it[k];
         if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
         double *res = decide ? acc : nullptr;
-        k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[0], t.nbr, t.nbr_n, t.rho, t.alpha,
+        k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[0], t.nbr, gsl, t.nbr_n, t.rho, t.alpha,
                                                     t.wg, t.kddiv.empty() ? kd : t.kddiv[0], nullptr, res);
         uint32_t it = 0;
         for (;;) {
@@ -1382,12 +1468,12 @@ struct AdjImpl : AdjBase {
                 break;
             }
             T *kd_t = t.kddiv[it];
-            k_m_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vdiv[it], t.vdiv[it + 1], t.nbr, t.nbr_n,
+            k_m_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vdiv[it], t.vdiv[it + 1], t.nbr, gsl, t.nbr_n,
                                                         kd_t, t.wg, nullptr, nullptr);
             ++it;
             if (decide || it < nd) {
                 if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
-                k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[it], t.nbr, t.nbr_n, t.rho,
+                k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[it], t.nbr, gsl, t.nbr_n, t.rho,
                                                             t.alpha, t.wg, t.kddiv[it], nullptr, res);
             }
         }
@@ -1396,14 +1482,14 @@ struct AdjImpl : AdjBase {
         k_m_forces_eval<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.vdiv[nd], t.nbr, t.nbr_n, t.rho, t.rhon,
                                                           t.pp, t.accel, t.blend, t.kdf, pressure);
         k_m_forces_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, f, c, t.x, t.vdiv[nd], t.vden[0], t.accel,
-                                                           t.blend, t.nbr, t.nbr_n, t.kdf, t.wg);
+                                                           t.blend, t.nbr, gsl, t.nbr_n, t.kdf, t.wg);
         // density loop
         const uint32_t ne = decide ? 0u : den_it[k];
         it = 0;
         for (;;) {
             if (!decide && it >= ne) break;
             if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
-            k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[it], t.nbr, t.nbr_n, t.rho,
+            k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[it], t.nbr, gsl, t.nbr_n, t.rho,
                                                         t.alpha, t.wg, t.kdden[it], pinc, res);
             if (decide) {
                 double r;
@@ -1411,7 +1497,7 @@ struct AdjImpl : AdjBase {
                 if (rc != FLUID_OK) return rc;
                 if (!(it < max_iters && r > (double)den_tol)) break;
             }
-            k_m_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vden[it], t.vden[it + 1], t.nbr, t.nbr_n,
+            k_m_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vden[it], t.vden[it + 1], t.nbr, gsl, t.nbr_n,
                                                         t.kdden[it], t.wg, pinc, pressure);
             ++it;
         }
