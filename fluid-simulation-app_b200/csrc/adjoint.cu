@@ -398,10 +398,22 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
             const uint32_t row = ((uint32_t)cz * p.dims[1] + (uint32_t)cy) * p.dims[0];
             uint32_t s = starts[row + cx0], e = starts[row + cx1 + 1];
             if (e > n) e = n;
-            for (uint32_t k = s; k < e; ++k) {
-                const uint32_t j = perm ? perm[k] : k;
-                if (j == i || j >= n) continue;
-                const V3<T> xij = xi - x[j];
+            // candidates four at a time: their positions load together
+            for (uint32_t k0 = s; k0 < e; k0 += 4) {
+                uint32_t jj[4];
+                V3<T> xj[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const uint32_t k = k0 + u;
+                    const uint32_t jr = k < e ? (perm ? perm[k] : k) : i;
+                    jj[u] = jr;
+                    xj[u] = x[jr < n ? jr : i];
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                const uint32_t j = jj[u];
+                if (k0 + u >= e || j == i || j >= n) continue;
+                const V3<T> xij = xi - xj[u];
                 const T r2 = dot(xij, xij);
                 if (r2 >= p.sup2) continue;
                 const Radial<T> R = radial(p, r2);
@@ -416,6 +428,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
                     if (gsl) gsl[(size_t)cnt * n + i] = R.gs;
                 }
                 cnt++;
+                }
             }
         }
     nbr_n[i] = cnt < kModelCap ? cnt : kModelCap;
@@ -614,18 +627,22 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_forces_eval(MP<T> p, uint32_t
     const T rho_i = rho[i], near_i = rhon[i];
     const uint32_t cnt = nbr_n[i];
     V3<T> visc = zero3<T>(), bl = zero3<T>(), near = zero3<T>(), ten = zero3<T>();
-    for (uint32_t k = 0; k < cnt; ++k) {
-        const uint32_t j = nbr[(size_t)k * n + i];
-        const V3<T> xij = xi - x[j];
+    struct Rec {
+        V3<T> x, v;
+        T rho, near;
+    };
+    rwalk<kRB, Rec>(nbr, n, i, cnt, [&](uint32_t j) { return Rec{x[j], v[j], rho[j], rhon[j]}; },
+                    [&](uint32_t, const Rec &q) {
+        const V3<T> xij = xi - q.x;
         const T r2 = dot(xij, xij);
         const Radial<T> R = radial(p, r2);
-        const T rho_j = rho[j];
+        const T rho_j = q.rho;
         const T f = R.gs * r2 / (r2 + p.eps);
         const T pair = p.m / (rho_i * rho_j) * f;
-        const V3<T> dv = vi - v[j];
+        const V3<T> dv = vi - q.v;
         const T wn = R.q < T(1) ? T(1) - R.q : T(0);
         const T rr = R.r > T(1e-5f) ? R.r : T(1e-5f);
-        near = near + ((near_i + rhon[j]) * wn * wn / rr) * xij;
+        near = near + ((near_i + q.near) * wn * wn / rr) * xij;
         visc = visc + (p.visc_k * pair) * dv;
         bl = bl - (p.m / rho_j * R.W) * dv;
         T C = T(0);
@@ -637,7 +654,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_forces_eval(MP<T> p, uint32_t
         const T corr = T(2) * p.rho0 / (rho_i + rho_j);
         const T rt = R.r > T(1e-9f) ? R.r : T(1e-9f);
         ten = ten - (corr * p.m * C / rt) * xij;
-    }
+    });
     V3<T> ad;
     w_adh<T, T>(p, xi.x, xi.y, xi.z, ad.x, ad.y, ad.z);
     accel[i] = visc + p.k_near * near + p.gamma * ten + (p.beta * p.rho0) * ad;
