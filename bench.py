@@ -58,10 +58,10 @@ ALGO_BYTES = {"grid": 20.0, "gather": 116.0, "density_div": 44.0, "div_kappa": 2
 # DRAM bytes (read + write) per particle per launch, from ncu captures of
 # each kernel on this workload at its full 1,048,576 particles
 # (profiles/list_sweeps_tilt_1m.md, profiles/density_div_tilt_1m.md).
-NCU_TRAFFIC_PER_PARTICLE = {"den_kappa": (583.2e6 + 5.2e6) / 1048576,
-                            "den_apply": (587.4e6 + 6.7e6) / 1048576,
-                            "div_apply": (587.4e6 + 6.7e6) / 1048576,
-                            "density_div": (66.9e6 + 484.9e6) / 1048576}
+NCU_TRAFFIC_PER_PARTICLE = {"den_kappa": (583.2e6 + 19.4e6) / 1048576,
+                            "den_apply": (604.1e6 + 15.5e6) / 1048576,
+                            "div_apply": (604.1e6 + 15.5e6) / 1048576,
+                            "density_div": (71.9e6 + 505.6e6) / 1048576}
 
 
 def load(name, path):
