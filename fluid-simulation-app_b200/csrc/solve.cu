@@ -527,11 +527,19 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
                             const uint32_t ku = k + u;
                             pc[u] = __ldg(&b.wpos[ku < e ? ku : i]);
                         }
+                        // every squared distance first, then the tests: the
+                        // candidates' arithmetic overlaps (0.88 -> 0.82 ms
+                        // against testing each as it is formed)
+                        float r2[FCU_DD_CHUNK];
+#pragma unroll
+                        for (int u = 0; u < FCU_DD_CHUNK; ++u) {
+                            const F3 x = pos - xyz(pc[u]);
+                            r2[u] = dot(x, x);
+                        }
 #pragma unroll
                         for (int u = 0; u < FCU_DD_CHUNK; ++u) {
                             const uint32_t ku = k + u;
-                            const F3 x = pos - xyz(pc[u]);
-                            if (ku < e && ku != i && dot(x, x) < P.support_sq) {
+                            if (ku < e && ku != i && r2[u] < P.support_sq) {
                                 s_hit[staged][tid] = (uint16_t)((r << 12) | (ku - rs));
                                 ++staged;
                             }
