@@ -273,7 +273,12 @@ class Adjoint:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module's globals may already be gone; the
+        # process's CUDA context goes with it
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     def forward(self, forces, xsph, target):
         f = np.ascontiguousarray(forces, np.float64).reshape(self.frames, 3)
@@ -331,7 +336,12 @@ class Batch:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module's globals may already be gone; the
+        # process's CUDA context goes with it
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     def params(self, box):
         p = FluidSimParams()
@@ -420,7 +430,12 @@ class Sim:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module's globals may already be gone; the
+        # process's CUDA context goes with it
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     def __enter__(self):
         return self
@@ -551,7 +566,12 @@ class Controller:
             self.h = None
 
     def __del__(self):
-        self.close()
+        # at interpreter exit the module's globals may already be gone; the
+        # process's CUDA context goes with it
+        try:
+            self.close()
+        except (TypeError, AttributeError):
+            pass
 
     def touch(self, slot, x, y, down):
         check(lib().fluid_controller_touch(self.h, slot, x, y, 1 if down else 0), "touch")
