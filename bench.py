@@ -22,6 +22,9 @@ GPU (a single box does not shard), max over ranks.
 batched: the batched-boxes workload (256 boxes, ~5.7M particles) as one
 batch per GPU; with N > 1 the boxes are LPT-sharded across the ranks
 (strong scaling, no collective in the step), device time max over ranks.
+At N = 1 the same boxes are also stepped by the plain step, one Sim per box,
+over the batch's first timed substeps (one box at a time, and all boxes on
+their own streams at once), for the batch-over-plain ratio.
 
 adjoint: the adjoint workload (65,536 particles, 120 frames): one forward
 and one backward of the differentiable model, timed on the device, next to
@@ -369,11 +372,15 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    e2 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    batch.run(steps[nw:])
+    batch.run(steps[nw:nw + PLAIN_BOX_SUBSTEPS])
     e1.record(stream)
-    e1.synchronize()
-    ms = e0.elapsed_time(e1)
+    batch.run(steps[nw + PLAIN_BOX_SUBSTEPS:])
+    e2.record(stream)
+    e2.synchronize()
+    ms = e0.elapsed_time(e2)
+    ms_head = e0.elapsed_time(e1)
     after = batch.stats()
     batch.reduce_stats()
     final = batch.stats()
@@ -389,6 +396,9 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     total = int(sum(counts))
     value = total * sub / (ms / 1000.0)
     batch.close()
+    plain_boxes = None
+    if world == 1 and not args.no_plain_boxes:
+        plain_boxes = plain_boxes_leg(fcu, cfgs, steps, nw, total * PLAIN_BOX_SUBSTEPS / (ms_head / 1000.0))
     return {"workload": "batched_256", "boxes": len(cfgs_all), "particles": total,
             "substeps": sub, "warmup_substeps": nw, "ms_per_substep": ms / sub, "value": value,
             "unit": UNIT, "sharding": f"LPT over {world} rank(s)" if world > 1 else "one batch",
@@ -398,9 +408,49 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
             "compression_avg_mean": float(rows[:, 2].mean()),
             "compression_avg_worst_box": float(rows[:, 2].max()),
             "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu,
+            "vs_the_same_boxes_as_plain_sims": plain_boxes,
             "autotuned_blocks": chosen,
             "autotune_ms_by_block": {str(t): dict(zip(fcu.Batch.TUNED, [round(float(x), 4) for x in tune_ms[c]]))
                                      for c, t in enumerate((64, 128, 256))}}
+
+
+PLAIN_BOX_SUBSTEPS = 12
+
+
+def plain_boxes_leg(fcu, cfgs, steps, nw, batch_value):
+    """The batched workload's boxes stepped by the plain step: one Sim per
+    box (fluid_sim_*), warmed up over the same substeps as the batch, then
+    the batch's first PLAIN_BOX_SUBSTEPS timed substeps, (a) one box after
+    another, each box's substeps then a device sync, and (b) every box's
+    substeps enqueued on its own stream, then one sync. Wall clock around
+    device syncs (the work spans 256 streams). Same Step blocks and the same
+    per-box results (each box bit-identical to the batch's)."""
+    import torch
+    sims = [fcu.Sim(c) for c in cfgs]
+    try:
+        counts = [s.n for s in sims]
+        for b, s in enumerate(sims):
+            s.run([row[b] for row in steps[:nw]])
+        torch.cuda.synchronize()
+        timed = steps[nw:nw + PLAIN_BOX_SUBSTEPS]
+        t0 = time.perf_counter()
+        for b, s in enumerate(sims):
+            s.run([row[b] for row in timed])
+            s.sync()
+        t1 = time.perf_counter()
+        for b, s in enumerate(sims):
+            s.run([row[b] for row in timed])
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+    finally:
+        for s in sims:
+            s.close()
+    work = sum(counts) * len(timed)
+    one_by_one, concurrent = work / (t1 - t0), work / (t2 - t1)
+    return {"substeps": len(timed), "batch_on_these_substeps": batch_value,
+            "one_box_at_a_time": one_by_one, "all_boxes_on_own_streams": concurrent,
+            "batch_over_one_at_a_time": batch_value / one_by_one,
+            "batch_over_concurrent": batch_value / concurrent}
 
 
 ADJ_FRAMES = 120
@@ -575,6 +625,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-boxes leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
+    ap.add_argument("--no-plain-boxes", action="store_true",
+                    help="skip stepping the batched boxes as separate plain sims")
     ap.add_argument("--profile-substeps", type=int, default=0,
                     help="after the warm-up, run this many substeps as direct launches timed per kernel, then exit")
     args = ap.parse_args()
