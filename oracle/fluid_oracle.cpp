@@ -12,6 +12,13 @@
 //     evaluation); exp of a per-substep constant is libm expf on the host;
 //   - every global sum is exact: per-particle FP64 terms in 2^-28 fixed point,
 //     summed as 64-bit integers, so the total does not depend on order.
+//
+// The substep's arithmetic type is Real: float, the oracle above. Compiled
+// with -DOR_REAL=double the same source is the FP64 oracle (same algorithm,
+// same float constants, every operation in double) that the FP32 path's
+// errors are stated against; its C API still takes and returns float, plus
+// or_sim_get_state64 for the double state. (The tracer and field helpers
+// stay float in both.)
 #include "fluid_oracle.h"
 
 #include <algorithm>
@@ -23,7 +30,13 @@
 #include <omp.h>
 #endif
 
+#ifndef OR_REAL
+#define OR_REAL float
+#endif
+
 namespace {
+
+typedef OR_REAL Real;
 
 constexpr float kPi = 3.14159265358979323846f;
 constexpr float kRestDensity = 998.2f;                // sim.rs:6
@@ -50,25 +63,43 @@ constexpr float T_CHARGE = 4.0f;
 constexpr float HUGE_F = 1e30f;  // sim_solve.wgsl:792
 
 struct V3 {
-    float x, y, z;
+    Real x, y, z;
 };
-inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
+inline V3 v3(Real x, Real y, Real z) { return V3{x, y, z}; }
 inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
 inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
 inline V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
-inline V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
-inline V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-inline V3 operator/(V3 a, float s) { return v3(a.x / s, a.y / s, a.z / s); }
-inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline float length(V3 a) { return std::sqrt(dot(a, a)); }
+inline V3 operator*(Real s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
+inline V3 operator*(V3 a, Real s) { return v3(a.x * s, a.y * s, a.z * s); }
+inline V3 operator/(V3 a, Real s) { return v3(a.x / s, a.y / s, a.z / s); }
+inline Real dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline Real length(V3 a) { return std::sqrt(dot(a, a)); }
 inline V3 cross(V3 a, V3 b) {
     return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
 }
-inline float fmaxw(float a, float b) { return a > b ? a : b; }  // WGSL max, finite inputs
-inline float fminw(float a, float b) { return a < b ? a : b; }
-inline float clampw(float e, float lo, float hi) { return fminw(fmaxw(e, lo), hi); }
-inline float mixw(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+// WGSL max / min / clamp / mix (finite inputs), in the wider of the argument
+// types (float with float is the float expression itself).
+template <class A, class B>
+inline auto fmaxw(A a, B b) -> decltype(a + b) {
+    typedef decltype(a + b) T;
+    return (T)a > (T)b ? (T)a : (T)b;
+}
+template <class A, class B>
+inline auto fminw(A a, B b) -> decltype(a + b) {
+    typedef decltype(a + b) T;
+    return (T)a < (T)b ? (T)a : (T)b;
+}
+template <class A, class B, class C>
+inline auto clampw(A e, B lo, C hi) -> decltype(e + lo + hi) {
+    return fminw(fmaxw(e, lo), hi);
+}
+template <class A, class B, class C>
+inline auto mixw(A a, B b, C t) -> decltype(a + b + t) {
+    typedef decltype(a + b + t) T;
+    return (T)a * ((T)1 - (T)t) + (T)b * (T)t;
+}
 inline V3 load3(const float *p) { return v3(p[0], p[1], p[2]); }
+inline V3 load3(const double *p) { return v3((Real)p[0], (Real)p[1], (Real)p[2]); }
 
 // exp for per-particle arguments, shared definition with the CUDA path:
 // x = k ln2 + r by Cody-Waite (ln2 split in a 16-bit head and a tail),
@@ -96,6 +127,8 @@ float or_exp(float x) {
     return p * scale;
 }
 
+inline float exp_r(float x) { return or_exp(x); }
+
 inline uint32_t pcg(uint32_t x) {  // sim_tracers.wgsl:54-58
     uint32_t h = x * 747796405u + 2891336453u;
     h = ((h >> ((h >> 28u) + 4u)) ^ h) * 277803737u;
@@ -109,6 +142,124 @@ inline int64_t fx(double term) {
     if (!(term > 0.0)) return 0;
     if (term > 16.0) term = 16.0;
     return (int64_t)std::llrint(term * kFixedScale);
+}
+
+// exp of a per-particle argument: or_exp in the float oracle, libm in the
+// FP64 one.
+inline float exp_r(float x);
+inline double exp_r(double x) { return std::exp(x); }
+
+// WGSL's f32 -> u32 saturating conversion, and the grid's cell and stable
+// counting sort over positions of either width (sim.rs:38-44;
+// sim_grid.wgsl:36-58; sim_scan.wgsl:97-120).
+template <class T>
+inline uint32_t sat_u32_t(T v) {
+    if (!(v > (T)0.0f)) return 0u;
+    if (v >= (T)4294967296.0f) return 0xffffffffu;
+    return (uint32_t)v;
+}
+template <class T>
+uint32_t cell_of_t(const OrGrid *g, const T *pos) {
+    uint32_t c[3];
+    for (int i = 0; i < 3; ++i) {
+        const uint32_t u = sat_u32_t((pos[i] - g->min[i]) / g->cell);
+        c[i] = u < g->dims[i] - 1u ? u : g->dims[i] - 1u;
+    }
+    return (c[2] * g->dims[1] + c[1]) * g->dims[0] + c[0];
+}
+template <class T>
+void grid_build_t(const OrGrid *g, const T *pos4, uint32_t n, uint32_t *keys, uint32_t *starts,
+                  uint32_t *perm) {
+    const uint32_t cells = g->dims[0] * g->dims[1] * g->dims[2];
+    std::vector<uint32_t> counts(cells, 0u);
+    std::vector<uint32_t> k(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        k[i] = cell_of_t(g, pos4 + 4 * (size_t)i);
+        counts[k[i]]++;
+    }
+    uint32_t run = 0;
+    for (uint32_t c = 0; c < cells; ++c) {
+        starts[c] = run;
+        run += counts[c];
+    }
+    starts[cells] = run;
+    for (uint32_t c = 0; c < cells; ++c) counts[c] = starts[c];
+    for (uint32_t i = 0; i < n; ++i) perm[counts[k[i]]++] = i;
+    if (keys) std::memcpy(keys, k.data(), sizeof(uint32_t) * n);
+}
+
+// A field of the substep as float.
+template <class V>
+void copy_out(void *out, const V &v) {
+    float *o = (float *)out;
+    for (size_t k = 0; k < v.size(); ++k) o[k] = (float)v[k];
+}
+
+// The wall and wedge polynomials (sim_solve.wgsl:213-235, :249-293, :334-340)
+// over the substep's Real; the exported float functions below are the
+// float instances.
+template <class T>
+T wall_density_t(T t) {
+    if (t >= 2.0f) return 0.0f;
+    const T t3 = t * t * t;
+    if (t < 1.0f) return 0.5f - 0.7f * t + t3 * (1.0f / 3.0f + t * t * (-0.15f + 0.05f * t));
+    return 8.0f / 15.0f - 0.8f * t + t3 * (2.0f / 3.0f + t * (-0.5f + t * (0.15f - t / 60.0f)));
+}
+template <class T>
+T wall_gradient_t(T t) {
+    if (t >= 2.0f) return 0.0f;
+    const T t2 = t * t;
+    if (t < 1.0f) return 0.7f + t2 * (-1.0f + t2 * (0.75f - t * 0.3f));
+    return 0.8f + t2 * (-2.0f + t * (2.0f + t * (-0.75f + t * 0.1f)));
+}
+template <class T>
+T wedge_t(T t1, T t2) {
+    if (t1 * t1 + t2 * t2 >= 4.0f) return 0.0f;
+    return (2.5005807e-01f +
+            t2 * (-3.4681153e-01f +
+                  t2 * (-4.0986882e-02f +
+                        t2 * (3.0301620e-01f +
+                              t2 * (-1.9202736e-01f + t2 * (4.6947582e-02f + t2 * (-3.8543515e-03f))))))) +
+           t1 * ((-3.4681153e-01f +
+                  t2 * (4.8587248e-01f +
+                        t2 * (1.0092180e-02f +
+                              t2 * (-2.9978363e-01f + t2 * (1.5320335e-01f + t2 * (-2.2544282e-02f)))))) +
+                 t1 * ((-4.0986882e-02f +
+                        t2 * (1.0092180e-02f +
+                              t2 * (-5.4145610e-02f + t2 * (7.9597369e-02f + t2 * (-2.3350373e-02f))))) +
+                       t1 * ((3.0301620e-01f +
+                              t2 * (-2.9978363e-01f + t2 * (7.9597369e-02f + t2 * (-8.2431946e-03f)))) +
+                             t1 * ((-1.9202736e-01f + t2 * (1.5320335e-01f + t2 * (-2.3350373e-02f))) +
+                                   t1 * ((4.6947582e-02f + t2 * (-2.2544282e-02f)) +
+                                         t1 * (-3.8543515e-03f))))));
+}
+template <class T>
+T wedge_d_t(T t1, T t2) {
+    if (t1 * t1 + t2 * t2 >= 4.0f) return 0.0f;
+    return (-3.4611994e-01f +
+            t2 * (4.4757673e-01f +
+                  t2 * (1.1932939e-01f +
+                        t2 * (-4.6460101e-01f +
+                              t2 * (2.7637253e-01f + t2 * (-6.2846025e-02f + t2 * (4.3871652e-03f))))))) +
+           t1 * ((-6.3622823e-02f +
+                  t2 * (2.0521006e-01f +
+                        t2 * (-3.7311339e-01f +
+                              t2 * (3.7508155e-01f + t2 * (-1.6629713e-01f + t2 * (2.5030129e-02f)))))) +
+                 t1 * ((7.8352497e-01f +
+                        t2 * (-1.2658344e+00f +
+                              t2 * (5.8898945e-01f + t2 * (-1.0772903e-01f + t2 * (1.3535777e-02f))))) +
+                       t1 * ((-4.9470084e-01f +
+                              t2 * (9.1302071e-01f + t2 * (-3.4330355e-01f + t2 * (2.4034609e-02f)))) +
+                             t1 * ((-2.5605481e-02f + t2 * (-2.0067981e-01f + t2 * (5.9854468e-02f))) +
+                                   t1 * ((8.8898623e-02f + t2 * (3.9914838e-03f)) +
+                                         t1 * (-1.7788321e-02f))))));
+}
+template <class T>
+T wall_adhesion_t(T t) {
+    const T u = clampw((T)2.0f - t, (T)0.0f, (T)2.0f);
+    return u * u *
+           (1.7847015e-3f +
+            u * (3.3392196e-3f + u * (-4.3394677e-3f + u * (1.6711868e-3f + u * (-2.1788750e-4f)))));
 }
 
 }  // namespace
@@ -140,20 +291,10 @@ float or_kernel(float r, float h) {
 
 // sim_solve.wgsl:213-222 (the runtime copy; sim.rs:261-272 is the same
 // polynomial in a different association and is checked by the tests)
-float or_wall_density(float t) {
-    if (t >= 2.0f) return 0.0f;
-    const float t3 = t * t * t;
-    if (t < 1.0f) return 0.5f - 0.7f * t + t3 * (1.0f / 3.0f + t * t * (-0.15f + 0.05f * t));
-    return 8.0f / 15.0f - 0.8f * t + t3 * (2.0f / 3.0f + t * (-0.5f + t * (0.15f - t / 60.0f)));
-}
+float or_wall_density(float t) { return wall_density_t<float>(t); }
 
 // sim_solve.wgsl:226-235
-float or_wall_gradient(float t) {
-    if (t >= 2.0f) return 0.0f;
-    const float t2 = t * t;
-    if (t < 1.0f) return 0.7f + t2 * (-1.0f + t2 * (0.75f - t * 0.3f));
-    return 0.8f + t2 * (-2.0f + t * (2.0f + t * (-0.75f + t * 0.1f)));
-}
+float or_wall_gradient(float t) { return wall_gradient_t<float>(t); }
 
 // sim.rs:296-316 (FP64, the tests' copy)
 double or_wedge64(double t1, double t2) {
@@ -209,56 +350,13 @@ double or_wall_adhesion64(double t) {
 }
 
 // sim_solve.wgsl:249-270
-float or_wedge(float t1, float t2) {
-    if (t1 * t1 + t2 * t2 >= 4.0f) return 0.0f;
-    return (2.5005807e-01f +
-            t2 * (-3.4681153e-01f +
-                  t2 * (-4.0986882e-02f +
-                        t2 * (3.0301620e-01f +
-                              t2 * (-1.9202736e-01f + t2 * (4.6947582e-02f + t2 * (-3.8543515e-03f))))))) +
-           t1 * ((-3.4681153e-01f +
-                  t2 * (4.8587248e-01f +
-                        t2 * (1.0092180e-02f +
-                              t2 * (-2.9978363e-01f + t2 * (1.5320335e-01f + t2 * (-2.2544282e-02f)))))) +
-                 t1 * ((-4.0986882e-02f +
-                        t2 * (1.0092180e-02f +
-                              t2 * (-5.4145610e-02f + t2 * (7.9597369e-02f + t2 * (-2.3350373e-02f))))) +
-                       t1 * ((3.0301620e-01f +
-                              t2 * (-2.9978363e-01f + t2 * (7.9597369e-02f + t2 * (-8.2431946e-03f)))) +
-                             t1 * ((-1.9202736e-01f + t2 * (1.5320335e-01f + t2 * (-2.3350373e-02f))) +
-                                   t1 * ((4.6947582e-02f + t2 * (-2.2544282e-02f)) +
-                                         t1 * (-3.8543515e-03f))))));
-}
+float or_wedge(float t1, float t2) { return wedge_t<float>(t1, t2); }
 
 // sim_solve.wgsl:272-293
-float or_wedge_d(float t1, float t2) {
-    if (t1 * t1 + t2 * t2 >= 4.0f) return 0.0f;
-    return (-3.4611994e-01f +
-            t2 * (4.4757673e-01f +
-                  t2 * (1.1932939e-01f +
-                        t2 * (-4.6460101e-01f +
-                              t2 * (2.7637253e-01f + t2 * (-6.2846025e-02f + t2 * (4.3871652e-03f))))))) +
-           t1 * ((-6.3622823e-02f +
-                  t2 * (2.0521006e-01f +
-                        t2 * (-3.7311339e-01f +
-                              t2 * (3.7508155e-01f + t2 * (-1.6629713e-01f + t2 * (2.5030129e-02f)))))) +
-                 t1 * ((7.8352497e-01f +
-                        t2 * (-1.2658344e+00f +
-                              t2 * (5.8898945e-01f + t2 * (-1.0772903e-01f + t2 * (1.3535777e-02f))))) +
-                       t1 * ((-4.9470084e-01f +
-                              t2 * (9.1302071e-01f + t2 * (-3.4330355e-01f + t2 * (2.4034609e-02f)))) +
-                             t1 * ((-2.5605481e-02f + t2 * (-2.0067981e-01f + t2 * (5.9854468e-02f))) +
-                                   t1 * ((8.8898623e-02f + t2 * (3.9914838e-03f)) +
-                                         t1 * (-1.7788321e-02f))))));
-}
+float or_wedge_d(float t1, float t2) { return wedge_d_t<float>(t1, t2); }
 
 // sim_solve.wgsl:334-340
-float or_wall_adhesion(float t) {
-    const float u = clampw(2.0f - t, 0.0f, 2.0f);
-    return u * u *
-           (1.7847015e-3f +
-            u * (3.3392196e-3f + u * (-4.3394677e-3f + u * (1.6711868e-3f + u * (-2.1788750e-4f)))));
-}
+float or_wall_adhesion(float t) { return wall_adhesion_t<float>(t); }
 
 // sim.rs:65-72
 void or_lattice_dims(float spacing, const float extent[2], float fill, uint32_t out[3]) {
@@ -415,41 +513,12 @@ void or_grid_box(const float lo[3], const float hi[3], float support, OrGrid *g)
     g->cell = support;
 }
 
-// sim.rs:38-44; sim_grid.wgsl:36-42. WGSL's f32 -> u32 saturates: negative
-// and NaN go to 0, values past u32 max go to u32 max.
-static inline uint32_t sat_u32(float v) {
-    if (!(v > 0.0f)) return 0u;
-    if (v >= 4294967296.0f) return 0xffffffffu;
-    return (uint32_t)v;
-}
-uint32_t or_cell_of(const OrGrid *g, const float pos[3]) {
-    uint32_t c[3];
-    for (int i = 0; i < 3; ++i) {
-        const uint32_t u = sat_u32((pos[i] - g->min[i]) / g->cell);
-        c[i] = u < g->dims[i] - 1u ? u : g->dims[i] - 1u;
-    }
-    return (c[2] * g->dims[1] + c[1]) * g->dims[0] + c[0];
-}
+uint32_t or_cell_of(const OrGrid *g, const float pos[3]) { return cell_of_t(g, pos); }
 
 // sim_grid.wgsl:44-58 + sim_scan.wgsl:97-120, with the stable order.
 void or_grid_build(const OrGrid *g, const float *pos4, uint32_t n, uint32_t *keys,
                    uint32_t *starts, uint32_t *perm) {
-    const uint32_t cells = g->dims[0] * g->dims[1] * g->dims[2];
-    std::vector<uint32_t> counts(cells, 0u);
-    std::vector<uint32_t> k(n);
-    for (uint32_t i = 0; i < n; ++i) {
-        k[i] = or_cell_of(g, pos4 + 4 * (size_t)i);
-        counts[k[i]]++;
-    }
-    uint32_t run = 0;
-    for (uint32_t c = 0; c < cells; ++c) {
-        starts[c] = run;
-        run += counts[c];
-    }
-    starts[cells] = run;
-    for (uint32_t c = 0; c < cells; ++c) counts[c] = starts[c];
-    for (uint32_t i = 0; i < n; ++i) perm[counts[k[i]]++] = i;
-    if (keys) std::memcpy(keys, k.data(), sizeof(uint32_t) * n);
+    grid_build_t(g, pos4, n, keys, starts, perm);
 }
 
 static void derive_kernel_consts(OrParams *p, float h) {
@@ -546,13 +615,13 @@ struct OrSim {
     OrParams p;
     uint32_t n, cells, ntr;
     // resting set (slot order of the last integrate) and working set
-    std::vector<float> pos, vel, pvel, pp, temp;  // pos/vel/pvel are float4
+    std::vector<Real> pos, vel, pvel, pp, temp;  // pos/vel/pvel are float4
     std::vector<uint32_t> id;
-    std::vector<float> wpos, wvel, wpvel, wpp, wtemp;
+    std::vector<Real> wpos, wvel, wpvel, wpp, wtemp;
     std::vector<uint32_t> wid;
     std::vector<uint32_t> keys, starts, perm;
-    std::vector<float> density, alpha, kd, pressure, pinc;
-    std::vector<float> accel, xsph, wgrad;  // float4
+    std::vector<Real> density, alpha, kd, pressure, pinc;
+    std::vector<Real> accel, xsph, wgrad;  // float4
     std::vector<uint32_t> nbr, nbr_n;       // nbr[k * n + i]
     uint32_t clamp_count, nbr_over;
     std::vector<uint32_t> tracers;
@@ -615,24 +684,40 @@ void or_sim_free(OrSim *s) { delete s; }
 void or_sim_set_state(OrSim *s, const float *pos4, const float *vel4, const float *prev_vel4,
                       const float *prev_p, const float *temp, const uint32_t *id) {
     const size_t n = s->n;
-    if (pos4) std::memcpy(s->pos.data(), pos4, 16 * n);
-    if (vel4) std::memcpy(s->vel.data(), vel4, 16 * n);
-    if (prev_vel4) std::memcpy(s->pvel.data(), prev_vel4, 16 * n);
-    if (prev_p) std::memcpy(s->pp.data(), prev_p, 4 * n);
-    if (temp) std::memcpy(s->temp.data(), temp, 4 * n);
+    auto in = [](std::vector<Real> &dst, const float *src, size_t m) {
+        if (src)
+            for (size_t k = 0; k < m; ++k) dst[k] = (Real)src[k];
+    };
+    in(s->pos, pos4, 4 * n);
+    in(s->vel, vel4, 4 * n);
+    in(s->pvel, prev_vel4, 4 * n);
+    in(s->pp, prev_p, n);
+    in(s->temp, temp, n);
     if (id) std::memcpy(s->id.data(), id, 4 * n);
 }
 
 void or_sim_get_state(const OrSim *s, float *pos4, float *vel4, float *prev_vel4, float *prev_p,
                       float *temp, uint32_t *id) {
     const size_t n = s->n;
-    if (pos4) std::memcpy(pos4, s->pos.data(), 16 * n);
-    if (vel4) std::memcpy(vel4, s->vel.data(), 16 * n);
-    if (prev_vel4) std::memcpy(prev_vel4, s->pvel.data(), 16 * n);
-    if (prev_p) std::memcpy(prev_p, s->pp.data(), 4 * n);
-    if (temp) std::memcpy(temp, s->temp.data(), 4 * n);
+    auto out = [](float *dst, const std::vector<Real> &src, size_t m) {
+        if (dst)
+            for (size_t k = 0; k < m; ++k) dst[k] = (float)src[k];
+    };
+    out(pos4, s->pos, 4 * n);
+    out(vel4, s->vel, 4 * n);
+    out(prev_vel4, s->pvel, 4 * n);
+    out(prev_p, s->pp, n);
+    out(temp, s->temp, n);
     if (id) std::memcpy(id, s->id.data(), 4 * n);
 }
+
+void or_sim_get_state64(const OrSim *s, double *pos4, double *vel4) {
+    const size_t n = s->n;
+    for (size_t k = 0; pos4 && k < 4 * n; ++k) pos4[k] = (double)s->pos[k];
+    for (size_t k = 0; vel4 && k < 4 * n; ++k) vel4[k] = (double)s->vel[k];
+}
+
+int or_sim_real_bytes(void) { return (int)sizeof(Real); }
 
 void or_sim_set_tracers(OrSim *s, const uint32_t *packed2) {
     std::memcpy(s->tracers.data(), packed2, 8 * (size_t)s->ntr);
@@ -657,94 +742,94 @@ OrGrid grid_of(const OrParams &p) {
 // (sim_grid.wgsl:44-72, sim_scan.wgsl:97-120).
 void rebuild(OrSim *s) {
     const OrGrid g = grid_of(s->p);
-    or_grid_build(&g, s->pos.data(), s->n, s->keys.data(), s->starts.data(), s->perm.data());
+    grid_build_t(&g, s->pos.data(), s->n, s->keys.data(), s->starts.data(), s->perm.data());
     const int64_t n = s->n;
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
     for (int64_t k = 0; k < n; ++k) {
         const size_t i = s->perm[k];
-        std::memcpy(&s->wpos[4 * k], &s->pos[4 * i], 16);
-        std::memcpy(&s->wvel[4 * k], &s->vel[4 * i], 16);
-        std::memcpy(&s->wpvel[4 * k], &s->pvel[4 * i], 16);
+        std::memcpy(&s->wpos[4 * k], &s->pos[4 * i], 4 * sizeof(Real));
+        std::memcpy(&s->wvel[4 * k], &s->vel[4 * i], 4 * sizeof(Real));
+        std::memcpy(&s->wpvel[4 * k], &s->pvel[4 * i], 4 * sizeof(Real));
         s->wpp[k] = s->pp[i];
         s->wtemp[k] = s->temp[i];
         s->wid[k] = s->id[i];
     }
 }
 
-inline float kernel_q(const OrParams &p, float q) {  // sim_solve.wgsl:176-182
+inline Real kernel_q(const OrParams &p, Real q) {  // sim_solve.wgsl:176-182
     if (q < 1.0f) return p.sigma * (1.0f - 1.5f * q * q * (1.0f - 0.5f * q));
-    const float t = 2.0f - q;
+    const Real t = 2.0f - q;
     return p.sigma * 0.25f * t * t * t;
 }
 
-inline V3 grad_q(const OrParams &p, V3 x, float r, float q) {  // sim_solve.wgsl:184-196
+inline V3 grad_q(const OrParams &p, V3 x, Real r, Real q) {  // sim_solve.wgsl:184-196
     if (r < 1e-9f) return v3(0.f, 0.f, 0.f);
-    float dw;
+    Real dw;
     if (q < 1.0f) {
         dw = p.sigma_h * (-3.0f * q + 2.25f * q * q);
     } else {
-        const float t = 2.0f - q;
+        const Real t = 2.0f - q;
         dw = p.sigma_h * (-0.75f * t * t);
     }
     return (dw / r) * x;
 }
 
-inline float cohesion(float r, float c, float k, float near) {  // sim_solve.wgsl:201-210
+inline Real cohesion(Real r, Real c, Real k, Real near) {  // sim_solve.wgsl:201-210
     if (r >= c || r < 1e-9f) return 0.0f;
-    const float a = (c - r) * (c - r) * (c - r) * r * r * r;
+    const Real a = (c - r) * (c - r) * (c - r) * r * r * r;
     if (2.0f * r > c) return k * a;
     return k * (2.0f * a - near);
 }
 
-inline float wedge_dsum(float t, float a, float b, float c, float d) {  // :295-297
-    return or_wedge_d(t, a) + or_wedge_d(t, b) + or_wedge_d(t, c) + or_wedge_d(t, d);
+inline Real wedge_dsum(Real t, Real a, Real b, Real c, Real d) {  // :295-297
+    return wedge_d_t(t, a) + wedge_d_t(t, b) + wedge_d_t(t, c) + wedge_d_t(t, d);
 }
 
-inline float wedge_sum(V3 tl, V3 th) {  // sim_solve.wgsl:299-304
-    float w = or_wedge(tl.x, tl.y) + or_wedge(tl.x, th.y) + or_wedge(th.x, tl.y) +
-              or_wedge(th.x, th.y);
-    w += or_wedge(tl.x, tl.z) + or_wedge(tl.x, th.z) + or_wedge(th.x, tl.z) + or_wedge(th.x, th.z);
-    w += or_wedge(tl.y, tl.z) + or_wedge(tl.y, th.z) + or_wedge(th.y, tl.z) + or_wedge(th.y, th.z);
+inline Real wedge_sum(V3 tl, V3 th) {  // sim_solve.wgsl:299-304
+    Real w = wedge_t(tl.x, tl.y) + wedge_t(tl.x, th.y) + wedge_t(th.x, tl.y) +
+              wedge_t(th.x, th.y);
+    w += wedge_t(tl.x, tl.z) + wedge_t(tl.x, th.z) + wedge_t(th.x, tl.z) + wedge_t(th.x, th.z);
+    w += wedge_t(tl.y, tl.z) + wedge_t(tl.y, th.z) + wedge_t(th.y, tl.z) + wedge_t(th.y, th.z);
     return w;
 }
 
 V3 wall_grad_sum(const OrParams &p, V3 pos) {  // sim_solve.wgsl:310-328
     const V3 lo = load3(p.wall_lo), hi = load3(p.wall_hi);
-    const float inv_h = 1.0f / p.h;
+    const Real inv_h = 1.0f / p.h;
     const V3 tl = (pos - lo) * inv_h;
     const V3 th = (hi - pos) * inv_h;
-    const float scale = p.rho0 * inv_h;
+    const Real scale = p.rho0 * inv_h;
     V3 g = v3(0.f, 0.f, 0.f);
-    g.x -= scale * (or_wall_gradient(tl.x) + wedge_dsum(tl.x, tl.y, th.y, tl.z, th.z));
-    g.x += scale * (or_wall_gradient(th.x) + wedge_dsum(th.x, tl.y, th.y, tl.z, th.z));
-    g.y -= scale * (or_wall_gradient(tl.y) + wedge_dsum(tl.y, tl.x, th.x, tl.z, th.z));
-    g.y += scale * (or_wall_gradient(th.y) + wedge_dsum(th.y, tl.x, th.x, tl.z, th.z));
-    g.z -= scale * (or_wall_gradient(tl.z) + wedge_dsum(tl.z, tl.x, th.x, tl.y, th.y));
-    g.z += scale * (or_wall_gradient(th.z) + wedge_dsum(th.z, tl.x, th.x, tl.y, th.y));
+    g.x -= scale * (wall_gradient_t(tl.x) + wedge_dsum(tl.x, tl.y, th.y, tl.z, th.z));
+    g.x += scale * (wall_gradient_t(th.x) + wedge_dsum(th.x, tl.y, th.y, tl.z, th.z));
+    g.y -= scale * (wall_gradient_t(tl.y) + wedge_dsum(tl.y, tl.x, th.x, tl.z, th.z));
+    g.y += scale * (wall_gradient_t(th.y) + wedge_dsum(th.y, tl.x, th.x, tl.z, th.z));
+    g.z -= scale * (wall_gradient_t(tl.z) + wedge_dsum(tl.z, tl.x, th.x, tl.y, th.y));
+    g.z += scale * (wall_gradient_t(th.z) + wedge_dsum(th.z, tl.x, th.x, tl.y, th.y));
     return g;
 }
 
 V3 wall_adh_sum(const OrParams &p, V3 pos) {  // sim_solve.wgsl:349-361
     const V3 lo = load3(p.wall_lo), hi = load3(p.wall_hi);
-    const float inv_h = 1.0f / p.h;
+    const Real inv_h = 1.0f / p.h;
     V3 a = v3(0.f, 0.f, 0.f);
-    a.x -= or_wall_adhesion((pos.x - lo.x) * inv_h);
-    a.x += or_wall_adhesion((hi.x - pos.x) * inv_h);
-    a.y -= or_wall_adhesion((pos.y - lo.y) * inv_h);
-    a.y += or_wall_adhesion((hi.y - pos.y) * inv_h);
-    a.z -= or_wall_adhesion((pos.z - lo.z) * inv_h);
-    a.z += or_wall_adhesion((hi.z - pos.z) * inv_h);
+    a.x -= wall_adhesion_t((pos.x - lo.x) * inv_h);
+    a.x += wall_adhesion_t((hi.x - pos.x) * inv_h);
+    a.y -= wall_adhesion_t((pos.y - lo.y) * inv_h);
+    a.y += wall_adhesion_t((hi.y - pos.y) * inv_h);
+    a.z -= wall_adhesion_t((pos.z - lo.z) * inv_h);
+    a.z += wall_adhesion_t((hi.z - pos.z) * inv_h);
     return a;
 }
 
-inline uint32_t base_coord(const OrParams &p, float v, int axis) {  // :363-368
-    const uint32_t u = sat_u32((v - p.box_min[axis]) / p.cell);
+inline uint32_t base_coord(const OrParams &p, Real v, int axis) {  // :363-368
+    const uint32_t u = sat_u32_t((v - p.box_min[axis]) / p.cell);
     return u < p.dims[axis] - 1u ? u : p.dims[axis] - 1u;
 }
 
 // density_div, sim_solve.wgsl:411-518. Returns the divergence residual
 // term sum (fixed point) of max(drho, 0) dt / rho0.
-int64_t density_div(OrSim *s, float dt) {
+int64_t density_div(OrSim *s, Real dt) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
     const uint32_t cap = p.nbr_cap;
@@ -756,11 +841,11 @@ int64_t density_div(OrSim *s, float dt) {
         const V3 vel = load3(&s->wvel[4 * pi]);
         const uint32_t bx = base_coord(p, pos.x, 0), by = base_coord(p, pos.y, 1),
                        bz = base_coord(p, pos.z, 2);
-        float w_sum = p.sigma;
-        float rho_near = 0.0f;
+        Real w_sum = p.sigma;
+        Real rho_near = 0.0f;
         V3 grad_sum = v3(0.f, 0.f, 0.f);
-        float grad_sq = 0.0f;
-        float drho = 0.0f;
+        Real grad_sq = 0.0f;
+        Real drho = 0.0f;
         uint32_t found = 0;
         for (int cell = 0; cell < 27; ++cell) {
             const int cx = (int)bx + (cell % 3) - 1;
@@ -774,12 +859,12 @@ int64_t density_div(OrSim *s, float dt) {
             for (uint32_t k = s->starts[c]; k < end; ++k) {
                 if ((int64_t)k == pi) continue;
                 const V3 x = pos - load3(&s->wpos[4 * (size_t)k]);
-                const float r2 = dot(x, x);
+                const Real r2 = dot(x, x);
                 if (r2 >= p.support_sq) continue;
-                const float r = std::sqrt(r2);
-                const float q = r * p.inv_h;
+                const Real r = std::sqrt(r2);
+                const Real q = r * p.inv_h;
                 w_sum += kernel_q(p, q);
-                const float wn = fmaxw(1.0f - q, 0.0f);
+                const Real wn = fmaxw(1.0f - q, 0.0f);
                 rho_near += wn * wn * wn;
                 const V3 gw = grad_q(p, x, r, q);
                 grad_sum = grad_sum + gw;
@@ -791,17 +876,17 @@ int64_t density_div(OrSim *s, float dt) {
         }
         s->nbr_n[pi] = found < cap ? found : cap;
         if (found > cap) over += found - cap;
-        float rho = p.mass * w_sum;
+        Real rho = p.mass * w_sum;
         grad_sq = p.mass * p.mass * grad_sq;
         drho = p.mass * drho;
         grad_sum = p.mass * grad_sum;
         const V3 lo = load3(p.wall_lo), hi = load3(p.wall_hi);
         const V3 tl = (pos - lo) * p.inv_h;
         const V3 th = (hi - pos) * p.inv_h;
-        float fill = 0.0f;
-        fill += or_wall_density(tl.x) + or_wall_density(th.x);
-        fill += or_wall_density(tl.y) + or_wall_density(th.y);
-        fill += or_wall_density(tl.z) + or_wall_density(th.z);
+        Real fill = 0.0f;
+        fill += wall_density_t(tl.x) + wall_density_t(th.x);
+        fill += wall_density_t(tl.y) + wall_density_t(th.y);
+        fill += wall_density_t(tl.z) + wall_density_t(th.z);
         fill -= wedge_sum(tl, th);
         rho += p.rho0 * fill;
         const V3 wg = wall_grad_sum(p, pos);
@@ -812,7 +897,7 @@ int64_t density_div(OrSim *s, float dt) {
         grad_sum = grad_sum + wg;
         s->density[pi] = rho;
         s->wpos[4 * pi + 3] = rho_near;
-        const float a = rho / fmaxw(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
+        const Real a = rho / fmaxw(dot(grad_sum, grad_sum) + grad_sq, 1e-4f);
         s->alpha[pi] = a;
         drho += dot(vel, wg);
         s->kd[pi] = fmaxw(drho, 0.0f) * a / fmaxw(dt, 1e-9f) / rho;
@@ -825,9 +910,9 @@ int64_t density_div(OrSim *s, float dt) {
 // Neighbour gradient, recomputed bit-for-bit as density_div wrote it.
 inline V3 nbr_grad(const OrSim *s, V3 pos, uint32_t j) {
     const V3 x = pos - load3(&s->wpos[4 * (size_t)j]);
-    const float r2 = dot(x, x);
-    const float r = std::sqrt(r2);
-    const float q = r * s->p.inv_h;
+    const Real r2 = dot(x, x);
+    const Real r = std::sqrt(r2);
+    const Real q = r * s->p.inv_h;
     return grad_q(s->p, x, r, q);
 }
 
@@ -835,7 +920,7 @@ inline V3 nbr_grad(const OrSim *s, V3 pos, uint32_t j) {
 inline V3 kappa_sum(const OrSim *s, int64_t pi, V3 pos) {
     const int64_t n = s->n;
     const uint32_t cnt = s->nbr_n[pi];
-    const float kd_i = s->kd[pi];
+    const Real kd_i = s->kd[pi];
     V3 dv = v3(0.f, 0.f, 0.f);
     for (uint32_t k = 0; k < cnt; ++k) {
         const uint32_t j = s->nbr[(size_t)k * n + pi];
@@ -847,10 +932,10 @@ inline V3 kappa_sum(const OrSim *s, int64_t pi, V3 pos) {
 
 // apply_kappa_wide (div_apply / den_apply), sim_solve.wgsl:608-621, and the
 // applied pressure kappa*rho for the density iterations.
-void apply_kappa(OrSim *s, float dt, bool add_pressure) {
+void apply_kappa(OrSim *s, Real dt, bool add_pressure) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
-    std::vector<float> out(4 * (size_t)n);
+    std::vector<Real> out(4 * (size_t)n);
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
     for (int64_t pi = 0; pi < n; ++pi) {
         const V3 pos = load3(&s->wpos[4 * pi]);
@@ -870,7 +955,7 @@ void apply_kappa(OrSim *s, float dt, bool add_pressure) {
 
 // The divergence predictor for a second or later divergence iteration: the
 // density_div sums again over the list, with this iteration's velocities.
-int64_t div_kappa(OrSim *s, float dt) {
+int64_t div_kappa(OrSim *s, Real dt) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
     int64_t res = 0;
@@ -879,7 +964,7 @@ int64_t div_kappa(OrSim *s, float dt) {
         const V3 pos = load3(&s->wpos[4 * pi]);
         const V3 vel = load3(&s->wvel[4 * pi]);
         const uint32_t cnt = s->nbr_n[pi];
-        float drho = 0.0f;
+        Real drho = 0.0f;
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t j = s->nbr[(size_t)k * n + pi];
             const V3 e = nbr_grad(s, pos, j);
@@ -887,7 +972,7 @@ int64_t div_kappa(OrSim *s, float dt) {
         }
         drho = p.mass * drho;
         drho += dot(vel, load3(&s->wgrad[4 * pi]));
-        const float rho = s->density[pi];
+        const Real rho = s->density[pi];
         s->kd[pi] = fmaxw(drho, 0.0f) * s->alpha[pi] / fmaxw(dt, 1e-9f) / rho;
         res += fx((double)fmaxw(drho, 0.0f) * (double)dt / (double)p.rho0);
     }
@@ -898,46 +983,46 @@ int64_t div_kappa(OrSim *s, float dt) {
 void forces_eval(OrSim *s) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
-    const float coh_c = 2.0f * p.h;
-    const float c3 = coh_c * coh_c * coh_c;
-    const float coh_k = 32.0f / (3.14159265f * c3 * c3 * c3);
-    const float coh_near = c3 * c3 / 64.0f;
-    const float c = 2.0f * p.h;
-    const float gamma = SIGMA_WATER * 7040.0f / (21.0f * LATTICE_SIGMA * p.rho0 * p.rho0 * c * c);
-    const float beta =
+    const Real coh_c = 2.0f * p.h;
+    const Real c3 = coh_c * coh_c * coh_c;
+    const Real coh_k = 32.0f / (3.14159265f * c3 * c3 * c3);
+    const Real coh_near = c3 * c3 / 64.0f;
+    const Real c = 2.0f * p.h;
+    const Real gamma = SIGMA_WATER * 7040.0f / (21.0f * LATTICE_SIGMA * p.rho0 * p.rho0 * c * c);
+    const Real beta =
         SIGMA_WATER * (1.0f + COS_CONTACT) * 1558.4f / (LATTICE_SIGMA * p.rho0 * p.rho0 * c * c);
-    const float visc_k = 2.0f * DYNAMIC_VISCOSITY;
-    const float heat_k = 2.0f * CONDUCTIVITY / HEAT_CAPACITY;
-    const float diss_k = 0.5f * DYNAMIC_VISCOSITY / HEAT_CAPACITY;
+    const Real visc_k = 2.0f * DYNAMIC_VISCOSITY;
+    const Real heat_k = 2.0f * CONDUCTIVITY / HEAT_CAPACITY;
+    const Real diss_k = 0.5f * DYNAMIC_VISCOSITY / HEAT_CAPACITY;
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
     for (int64_t pi = 0; pi < n; ++pi) {
-        const float *pos4 = &s->wpos[4 * pi];
+        const Real *pos4 = &s->wpos[4 * pi];
         const V3 pos = load3(pos4);
         const V3 vel = load3(&s->wvel[4 * pi]);
-        const float temp = s->wtemp[pi];
-        const float rho_i = s->density[pi];
+        const Real temp = s->wtemp[pi];
+        const Real rho_i = s->density[pi];
         const uint32_t cnt = s->nbr_n[pi];
         V3 visc = v3(0.f, 0.f, 0.f), blend = v3(0.f, 0.f, 0.f), near = v3(0.f, 0.f, 0.f),
            tension = v3(0.f, 0.f, 0.f);
-        float heat = 0.0f;
+        Real heat = 0.0f;
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t j = s->nbr[(size_t)k * n + pi];
             const V3 e = nbr_grad(s, pos, j);
-            const float *pj = &s->wpos[4 * (size_t)j];
+            const Real *pj = &s->wpos[4 * (size_t)j];
             const V3 x = pos - load3(pj);
-            const float r2 = dot(x, x);
-            const float r = std::sqrt(r2);
-            const float rho_j = s->density[j];
-            const float f = dot(x, e) / (r2 + 0.01f * p.h * p.h);
-            const float pair = p.mass / (rho_i * rho_j) * f;
+            const Real r2 = dot(x, x);
+            const Real r = std::sqrt(r2);
+            const Real rho_j = s->density[j];
+            const Real f = dot(x, e) / (r2 + 0.01f * p.h * p.h);
+            const Real pair = p.mass / (rho_i * rho_j) * f;
             const V3 dv = vel - load3(&s->wvel[4 * (size_t)j]);
-            const float wn = fmaxw(1.0f - r * p.inv_h, 0.0f);
+            const Real wn = fmaxw(1.0f - r * p.inv_h, 0.0f);
             near = near + ((pos4[3] + pj[3]) * wn * wn) * (x / fmaxw(r, 1e-5f));
             visc = visc + (visc_k * pair) * dv;
             blend = blend - (p.mass / rho_j * kernel_q(p, r * p.inv_h)) * dv;
             heat += heat_k * pair * (temp - s->wtemp[j]);
             heat -= diss_k * pair * dot(dv, dv);
-            const float corr = 2.0f * p.rho0 / (rho_i + rho_j);
+            const Real corr = 2.0f * p.rho0 / (rho_i + rho_j);
             tension = tension - ((corr * p.mass * cohesion(r, coh_c, coh_k, coh_near)) * x) /
                                     fmaxw(r, 1e-9f);
         }
@@ -951,8 +1036,8 @@ void forces_eval(OrSim *s) {
         s->xsph[4 * pi + 1] = blend.y;
         s->xsph[4 * pi + 2] = blend.z;
         s->xsph[4 * pi + 3] = 0.0f;
-        const float rho = s->density[pi];
-        const float half = 0.5f * s->wpp[pi];
+        const Real rho = s->density[pi];
+        const Real half = 0.5f * s->wpp[pi];
         s->kd[pi] = half / (rho * rho);
         s->pressure[pi] = half;
     }
@@ -960,34 +1045,34 @@ void forces_eval(OrSim *s) {
 
 // fingers, sim_solve.wgsl:103-127.
 V3 fingers(const OrStep &st, V3 pos, V3 v) {
-    float px = 0.0f, py = 0.0f, weight = 0.0f;
+    Real px = 0.0f, py = 0.0f, weight = 0.0f;
     for (uint32_t i = 0; i < st.touch_n && i < 5; ++i) {
         const float *t = st.touches[i];
-        const float dx = pos.x - t[0], dy = pos.y - t[1];
-        const float q2 = (dx * dx + dy * dy) / (st.touch_r * st.touch_r);
+        const Real dx = pos.x - t[0], dy = pos.y - t[1];
+        const Real q2 = (dx * dx + dy * dy) / (st.touch_r * st.touch_r);
         if (q2 < 1.0f) {
-            const float w = (1.0f - q2) * (1.0f - q2);
+            const Real w = (1.0f - q2) * (1.0f - q2);
             px += w * t[2];
             py += w * t[3];
             weight += w;
         }
     }
     if (weight <= 0.0f) return v;
-    const float a = 1.0f - or_exp(-TOUCH_RATE * weight * st.dt);
+    const Real a = 1.0f - exp_r(-TOUCH_RATE * weight * st.dt);
     return v3(mixw(v.x, px / weight, a), mixw(v.y, py / weight, a), v.z);
 }
 
 // forces_den_apply, sim_solve.wgsl:630-663.
-void forces_den_apply(OrSim *s, const OrStep &st, float xsph_blend) {
+void forces_den_apply(OrSim *s, const OrStep &st, Real xsph_blend) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
     const V3 force = load3(st.force), omega = load3(st.omega), domega = load3(st.domega);
-    std::vector<float> out(4 * (size_t)n);
+    std::vector<Real> out(4 * (size_t)n);
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
     for (int64_t pi = 0; pi < n; ++pi) {
         const V3 pos = load3(&s->wpos[4 * pi]);
         const V3 total = kappa_sum(s, pi, pos);
-        const float *a = &s->accel[4 * pi];
+        const Real *a = &s->accel[4 * pi];
         const V3 r = pos;
         const V3 v = load3(&s->wvel[4 * pi]);
         const V3 fict =
@@ -1008,7 +1093,7 @@ void forces_den_apply(OrSim *s, const OrStep &st, float xsph_blend) {
 // den_kappa, sim_solve.wgsl:674-698; the applied pressure k*rho is held in
 // pinc until den_apply applies the kappa it belongs to. Returns the density
 // residual sum (fixed point) of max(rho*/rho0 - 1, 0).
-int64_t den_kappa(OrSim *s, float dt) {
+int64_t den_kappa(OrSim *s, Real dt) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
     int64_t res = 0;
@@ -1017,16 +1102,16 @@ int64_t den_kappa(OrSim *s, float dt) {
         const V3 pos = load3(&s->wpos[4 * pi]);
         const V3 vel = load3(&s->wvel[4 * pi]);
         const uint32_t cnt = s->nbr_n[pi];
-        float drho = 0.0f;
+        Real drho = 0.0f;
         for (uint32_t k = 0; k < cnt; ++k) {
             const uint32_t j = s->nbr[(size_t)k * n + pi];
             const V3 e = nbr_grad(s, pos, j);
             drho += dot(vel - load3(&s->wvel[4 * (size_t)j]), e);
         }
-        const float rho = s->density[pi];
+        const Real rho = s->density[pi];
         drho = p.mass * drho + dot(vel, load3(&s->wgrad[4 * pi]));
-        const float rho_star = rho + dt * drho;
-        const float k = fmaxw(rho_star - p.rho0, 0.0f) * s->alpha[pi] / (dt * dt);
+        const Real rho_star = rho + dt * drho;
+        const Real k = fmaxw(rho_star - p.rho0, 0.0f) * s->alpha[pi] / (dt * dt);
         s->kd[pi] = k / rho;
         s->pinc[pi] = k * rho;
         res += fx((double)rho_star / (double)p.rho0 - 1.0);
@@ -1035,23 +1120,23 @@ int64_t den_kappa(OrSim *s, float dt) {
 }
 
 // integrate, sim_solve.wgsl:709-756, with the lens chase precomputed.
-void integrate(OrSim *s, const OrStep &st, float chase) {
+void integrate(OrSim *s, const OrStep &st, Real chase) {
     const OrParams &p = s->p;
     const int64_t n = s->n;
     const V3 lo = load3(p.wall_lo), hi = load3(p.wall_hi);
     uint32_t clamps = 0;
 #pragma omp parallel for num_threads(nthreads()) schedule(static) reduction(+ : clamps)
     for (int64_t i = 0; i < n; ++i) {
-        const float *was = &s->wvel[4 * i];
+        const Real *was = &s->wvel[4 * i];
         V3 v = load3(was);
-        const float speed = length(v);
-        const float ceiling = s->density[i] < 0.5f * p.rho0 ? 3.0f * st.v_clamp : st.v_clamp;
+        const Real speed = length(v);
+        const Real ceiling = s->density[i] < 0.5f * p.rho0 ? 3.0f * st.v_clamp : st.v_clamp;
         if (speed > ceiling) {
             v = v * (ceiling / speed);
             clamps++;
         }
-        const float *pv = &s->wpvel[4 * i];
-        const float accel = length(v - load3(pv)) / st.dt;
+        const Real *pv = &s->wpvel[4 * i];
+        const Real accel = length(v - load3(pv)) / st.dt;
         const V3 pp = load3(&s->wpos[4 * i]) + v * st.dt;
         const V3 cl = v3(clampw(pp.x, lo.x, hi.x), clampw(pp.y, lo.y, hi.y), clampw(pp.z, lo.z, hi.z));
         if (cl.x != pp.x) v.x = 0.0f;
@@ -1069,16 +1154,16 @@ void integrate(OrSim *s, const OrStep &st, float chase) {
         s->pvel[4 * i + 1] = v.y;
         s->pvel[4 * i + 2] = v.z;
         s->pvel[4 * i + 3] = mixw(pv[3], s->pressure[i], chase);
-        const float dp = s->pressure[i] - s->wpp[i];
+        const Real dp = s->pressure[i] - s->wpp[i];
         s->pp[i] = s->pressure[i];
-        const float t = s->wtemp[i];
+        const Real t = s->wtemp[i];
         s->temp[i] = t + t * EXPANSION / (s->density[i] * HEAT_CAPACITY) * dp;
         s->id[i] = s->wid[i];
     }
     s->clamp_count += clamps;
 }
 
-float step_xsph_blend(const OrParams &p, float dt) {
+Real step_xsph_blend(const OrParams &p, Real dt) {
     return p.xsph_blend >= 0.0f ? p.xsph_blend : 1.0f - std::exp(-XSPH_RATE * dt);
 }
 
@@ -1145,28 +1230,28 @@ void or_sim_stats(OrSim *s, float out[14]) {
     const OrParams &p = s->p;
     const size_t n = s->n;
     int64_t sum = 0;
-    float m = 0.0f, lo = HUGE_F, hi = -HUGE_F;
+    Real m = 0.0f, lo = HUGE_F, hi = -HUGE_F;
     for (size_t i = 0; i < n; ++i) {
-        const float c = s->density[i] / p.rho0 - 1.0f;
+        const Real c = s->density[i] / p.rho0 - 1.0f;
         sum += fx((double)fmaxw(c, 0.0f));
         m = fmaxw(m, c);
         lo = fminw(lo, s->density[i]);
         hi = fmaxw(hi, s->density[i]);
     }
-    out[0] = (float)((double)sum / kFixedScale / (double)n);
+    out[0] = (Real)((double)sum / kFixedScale / (double)n);
     out[1] = fmaxw(m, 0.0f);
     out[2] = lo;
     out[3] = hi;
-    float v_lo = HUGE_F, v_hi = -HUGE_F, a_lo = HUGE_F, a_hi = -HUGE_F;
-    float p_lo = HUGE_F, p_hi = -HUGE_F, t_lo = HUGE_F, t_hi = -HUGE_F;
+    Real v_lo = HUGE_F, v_hi = -HUGE_F, a_lo = HUGE_F, a_hi = -HUGE_F;
+    Real p_lo = HUGE_F, p_hi = -HUGE_F, t_lo = HUGE_F, t_hi = -HUGE_F;
     for (size_t i = 0; i < n; ++i) {
-        const float *q = &s->vel[4 * i];
-        const float speed = length(load3(q));
+        const Real *q = &s->vel[4 * i];
+        const Real speed = length(load3(q));
         v_lo = fminw(v_lo, speed);
         v_hi = fmaxw(v_hi, speed);
         a_lo = fminw(a_lo, q[3]);
         a_hi = fmaxw(a_hi, q[3]);
-        const float pr = s->pvel[4 * i + 3];
+        const Real pr = s->pvel[4 * i + 3];
         p_lo = fminw(p_lo, pr);
         p_hi = fmaxw(p_hi, pr);
         t_lo = fminw(t_lo, s->temp[i]);
@@ -1180,8 +1265,8 @@ void or_sim_stats(OrSim *s, float out[14]) {
     out[5] = p_hi;
     out[7] = t_lo;
     out[8] = t_hi;
-    out[9] = (float)s->clamp_count;
-    out[10] = (float)s->nbr_over;
+    out[9] = (Real)s->clamp_count;
+    out[10] = (Real)s->nbr_over;
 }
 
 namespace {
@@ -1252,9 +1337,9 @@ void or_sim_advect(OrSim *s, const OrStep *st) {  // sim_tracers.wgsl:140-183
         float old[4];
         load_tracer(s, i, old);
         V3 pos = v3(old[0], old[1], old[2]);
-        const float gp[3] = {(pos.x - p.box_min[0]) / p.cell - 0.5f,
-                             (pos.y - p.box_min[1]) / p.cell - 0.5f,
-                             (pos.z - p.box_min[2]) / p.cell - 0.5f};
+        const float gp[3] = {(float)((pos.x - p.box_min[0]) / p.cell - 0.5f),
+                             (float)((pos.y - p.box_min[1]) / p.cell - 0.5f),
+                             (float)((pos.z - p.box_min[2]) / p.cell - 0.5f)};
         uint32_t base[3];
         float f[3];
         for (int a = 0; a < 3; ++a) {
@@ -1301,8 +1386,8 @@ void or_sim_tracers(OrSim *s, const OrStep *st) {
     const OrGrid g = grid_of(p);
     // splat (sim_tracers.wgsl:98-114): integer sums, order-free
     for (size_t i = 0; i < s->n; ++i) {
-        const uint32_t c = or_cell_of(&g, &s->pos[4 * i]);
-        const float *v = &s->vel[4 * i];
+        const uint32_t c = cell_of_t(&g, &s->pos[4 * i]);
+        const Real *v = &s->vel[4 * i];
         int32_t *cell = &s->vel_grid[4 * (size_t)c];
         cell[0] = (int32_t)((uint32_t)cell[0] + (uint32_t)to_fixed(v[0]));
         cell[1] = (int32_t)((uint32_t)cell[1] + (uint32_t)to_fixed(v[1]));
@@ -1318,18 +1403,18 @@ void or_sim_tracers(OrSim *s, const OrStep *st) {
 void or_sim_field(const OrSim *s, int field, void *out) {
     const size_t n = s->n;
     switch (field) {
-    case OR_FIELD_DENSITY: std::memcpy(out, s->density.data(), 4 * n); break;
-    case OR_FIELD_ALPHA: std::memcpy(out, s->alpha.data(), 4 * n); break;
-    case OR_FIELD_KD: std::memcpy(out, s->kd.data(), 4 * n); break;
-    case OR_FIELD_PRESSURE: std::memcpy(out, s->pressure.data(), 4 * n); break;
+    case OR_FIELD_DENSITY: copy_out(out, s->density); break;
+    case OR_FIELD_ALPHA: copy_out(out, s->alpha); break;
+    case OR_FIELD_KD: copy_out(out, s->kd); break;
+    case OR_FIELD_PRESSURE: copy_out(out, s->pressure); break;
     case OR_FIELD_NBR_N: std::memcpy(out, s->nbr_n.data(), 4 * n); break;
     case OR_FIELD_STARTS: std::memcpy(out, s->starts.data(), 4 * (size_t)(s->cells + 1)); break;
     case OR_FIELD_PERM: std::memcpy(out, s->perm.data(), 4 * n); break;
-    case OR_FIELD_WORK_POS: std::memcpy(out, s->wpos.data(), 16 * n); break;
-    case OR_FIELD_WORK_VEL: std::memcpy(out, s->wvel.data(), 16 * n); break;
-    case OR_FIELD_ACCEL: std::memcpy(out, s->accel.data(), 16 * n); break;
-    case OR_FIELD_XSPH: std::memcpy(out, s->xsph.data(), 16 * n); break;
-    case OR_FIELD_WALL_GRAD: std::memcpy(out, s->wgrad.data(), 16 * n); break;
+    case OR_FIELD_WORK_POS: copy_out(out, s->wpos); break;
+    case OR_FIELD_WORK_VEL: copy_out(out, s->wvel); break;
+    case OR_FIELD_ACCEL: copy_out(out, s->accel); break;
+    case OR_FIELD_XSPH: copy_out(out, s->xsph); break;
+    case OR_FIELD_WALL_GRAD: copy_out(out, s->wgrad); break;
     case OR_FIELD_COUNTERS: {
         uint32_t *o = (uint32_t *)out;
         o[0] = s->clamp_count;

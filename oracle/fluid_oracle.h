@@ -136,6 +136,11 @@ void or_sim_substep(OrSim *s, const OrStep *st, uint32_t div_iters, uint32_t den
 /* One substep with tolerance-driven iteration counts (FP64 residuals). */
 void or_sim_substep_tol(OrSim *s, const OrStep *st, float div_tol, float den_tol,
                         uint32_t max_iters, uint32_t out_iters[2], double out_res[2]);
+/* The state in double: the FP64 oracle's own values (the float oracle's,
+ * widened). Either pointer may be null. */
+void or_sim_get_state64(const OrSim *s, double *pos4, double *vel4);
+/* sizeof the substep's arithmetic type: 4 (the oracle), 8 (the FP64 oracle). */
+int or_sim_real_bytes(void);
 /* reduce_stats into out[14] (sim_solve.wgsl:800-874). */
 void or_sim_stats(OrSim *s, float out[14]);
 /* One tracer pass (splat, resolve, advect), sim_tracers.wgsl. */

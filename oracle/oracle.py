@@ -11,6 +11,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libfluid_oracle.so")
+LIB64_PATH = os.path.join(HERE, "_build", "libfluid_oracle64.so")
 
 FIELD = dict(density=0, alpha=1, kd=2, pressure=3, nbr_n=4, starts=5, perm=6, work_pos=7,
              work_vel=8, accel=9, xsph=10, wall_grad=11, counters=12)
@@ -44,71 +45,88 @@ def build():
 
 
 _lib = None
+_lib64 = None
 
 
 def lib():
+    """The oracle (binary32, the CUDA path's bit-for-bit reference)."""
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
-        L = C.CDLL(LIB_PATH)
-        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
-        u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
-        F, U, D = C.c_float, C.c_uint32, C.c_double
-        sig = {
-            "or_hash": (U, [U]),
-            "or_kernel": (F, [F, F]),
-            "or_wall_density": (F, [F]),
-            "or_wall_gradient": (F, [F]),
-            "or_wedge64": (D, [D, D]),
-            "or_wedge_d64": (D, [D, D]),
-            "or_wall_adhesion64": (D, [D]),
-            "or_wedge": (F, [F, F]),
-            "or_wedge_d": (F, [F, F]),
-            "or_wall_adhesion": (F, [F]),
-            "or_half_bits": (C.c_uint16, [F]),
-            "or_half_value": (F, [C.c_uint16]),
-            "or_slab_depth": (F, []),
-            "or_rest_density": (F, []),
-            "or_cell_of": (U, [C.POINTER(OrGrid), f32p]),
-            "or_grid_slab": (None, [f32p, F, C.POINTER(OrGrid)]),
-            "or_grid_box": (None, [f32p, f32p, F, C.POINTER(OrGrid)]),
-            "or_grid_build": (None, [C.POINTER(OrGrid), f32p, U, C.c_void_p, u32p, u32p]),
-            "or_lattice_dims": (None, [F, f32p, F, u32p]),
-            "or_seed_slab": (U, [F, f32p, F, C.c_void_p]),
-            "or_seed_tracers": (None, [U, f32p, F, u32p]),
-            "or_seed_block": (U, [f32p, F, u32p, F, C.c_uint64, C.c_void_p]),
-            "or_pack_tracer": (None, [f32p, F, f32p, u32p]),
-            "or_unpack_tracer": (None, [u32p, f32p, f32p]),
-            "or_pack_step": (None, [f32p, f32p, f32p, F, F, U, U, F, C.c_void_p,
-                                    np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]),
-            "or_pack_sim_params": (None, [C.POINTER(OrGrid), U, F, F, F,
-                                          np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]),
-            "or_params_slab": (None, [f32p, F, F, U, C.POINTER(OrParams)]),
-            "or_params_box": (None, [f32p, f32p, F, F, F, U, C.POINTER(OrParams)]),
-            "or_sim_new": (C.c_void_p, [C.POINTER(OrParams), U]),
-            "or_sim_free": (None, [C.c_void_p]),
-            "or_sim_set_threads": (None, [C.c_int]),
-            "or_sim_set_state": (None, [C.c_void_p] + [C.c_void_p] * 6),
-            "or_sim_get_state": (None, [C.c_void_p] + [C.c_void_p] * 6),
-            "or_sim_set_tracers": (None, [C.c_void_p, u32p]),
-            "or_sim_get_tracers": (None, [C.c_void_p, u32p]),
-            "or_sim_substep": (None, [C.c_void_p, C.POINTER(OrStep), U, U]),
-            "or_sim_substep_tol": (None, [C.c_void_p, C.POINTER(OrStep), F, F, U, u32p,
-                                          np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]),
-            "or_sim_stats": (None, [C.c_void_p, f32p]),
-            "or_sim_tracers": (None, [C.c_void_p, C.POINTER(OrStep)]),
-            "or_sim_advect": (None, [C.c_void_p, C.POINTER(OrStep)]),
-            "or_sim_field": (None, [C.c_void_p, C.c_int, C.c_void_p]),
-            "or_field_splat": (None, [C.c_void_p] * 4 + [U, f32p, U, U, U, F, f32p]),
-            "or_field_filter": (None, [f32p, U, U, F, F, f32p]),
-        }
-        for name, (res, args) in sig.items():
-            fn = getattr(L, name)
-            fn.restype = res
-            fn.argtypes = args
-        _lib = L
+        _lib = load_library(LIB_PATH)
     return _lib
+
+
+def lib64():
+    """The FP64 oracle: the same source with every substep operation in
+    double (same C API, float in and out, plus or_sim_get_state64)."""
+    global _lib64
+    if _lib64 is None:
+        _lib64 = load_library(LIB64_PATH)
+    return _lib64
+
+
+def load_library(path):
+    if not os.path.exists(path):
+        build()
+    L = C.CDLL(path)
+    f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+    u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+    F, U, D = C.c_float, C.c_uint32, C.c_double
+    sig = {
+        "or_hash": (U, [U]),
+        "or_kernel": (F, [F, F]),
+        "or_wall_density": (F, [F]),
+        "or_wall_gradient": (F, [F]),
+        "or_wedge64": (D, [D, D]),
+        "or_wedge_d64": (D, [D, D]),
+        "or_wall_adhesion64": (D, [D]),
+        "or_wedge": (F, [F, F]),
+        "or_wedge_d": (F, [F, F]),
+        "or_wall_adhesion": (F, [F]),
+        "or_half_bits": (C.c_uint16, [F]),
+        "or_half_value": (F, [C.c_uint16]),
+        "or_slab_depth": (F, []),
+        "or_rest_density": (F, []),
+        "or_cell_of": (U, [C.POINTER(OrGrid), f32p]),
+        "or_grid_slab": (None, [f32p, F, C.POINTER(OrGrid)]),
+        "or_grid_box": (None, [f32p, f32p, F, C.POINTER(OrGrid)]),
+        "or_grid_build": (None, [C.POINTER(OrGrid), f32p, U, C.c_void_p, u32p, u32p]),
+        "or_lattice_dims": (None, [F, f32p, F, u32p]),
+        "or_seed_slab": (U, [F, f32p, F, C.c_void_p]),
+        "or_seed_tracers": (None, [U, f32p, F, u32p]),
+        "or_seed_block": (U, [f32p, F, u32p, F, C.c_uint64, C.c_void_p]),
+        "or_pack_tracer": (None, [f32p, F, f32p, u32p]),
+        "or_unpack_tracer": (None, [u32p, f32p, f32p]),
+        "or_pack_step": (None, [f32p, f32p, f32p, F, F, U, U, F, C.c_void_p,
+                                np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]),
+        "or_pack_sim_params": (None, [C.POINTER(OrGrid), U, F, F, F,
+                                      np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")]),
+        "or_params_slab": (None, [f32p, F, F, U, C.POINTER(OrParams)]),
+        "or_params_box": (None, [f32p, f32p, F, F, F, U, C.POINTER(OrParams)]),
+        "or_sim_new": (C.c_void_p, [C.POINTER(OrParams), U]),
+        "or_sim_free": (None, [C.c_void_p]),
+        "or_sim_set_threads": (None, [C.c_int]),
+        "or_sim_set_state": (None, [C.c_void_p] + [C.c_void_p] * 6),
+        "or_sim_get_state": (None, [C.c_void_p] + [C.c_void_p] * 6),
+        "or_sim_set_tracers": (None, [C.c_void_p, u32p]),
+        "or_sim_get_tracers": (None, [C.c_void_p, u32p]),
+        "or_sim_substep": (None, [C.c_void_p, C.POINTER(OrStep), U, U]),
+        "or_sim_substep_tol": (None, [C.c_void_p, C.POINTER(OrStep), F, F, U, u32p,
+                                      np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")]),
+        "or_sim_stats": (None, [C.c_void_p, f32p]),
+        "or_sim_tracers": (None, [C.c_void_p, C.POINTER(OrStep)]),
+        "or_sim_advect": (None, [C.c_void_p, C.POINTER(OrStep)]),
+        "or_sim_field": (None, [C.c_void_p, C.c_int, C.c_void_p]),
+        "or_field_splat": (None, [C.c_void_p] * 4 + [U, f32p, U, U, U, F, f32p]),
+        "or_field_filter": (None, [f32p, U, U, F, F, f32p]),
+        "or_sim_get_state64": (None, [C.c_void_p, C.c_void_p, C.c_void_p]),
+        "or_sim_real_bytes": (C.c_int, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
 
 
 def f32(a):
@@ -194,62 +212,71 @@ def params_box(lo, hi, spacing, h_ratio, rho0, count):
 
 
 class Sim:
-    """The oracle's substep over a resting set, in slot order."""
+    """The oracle's substep over a resting set, in slot order. fp64=True runs
+    the FP64 oracle (state() still returns float32; state64() the doubles);
+    library= a loaded oracle library of either kind."""
 
-    def __init__(self, params, tracers=0):
+    def __init__(self, params, tracers=0, fp64=False, library=None):
+        self.L = library if library is not None else (lib64() if fp64 else lib())
         self.p = params
         self.n = params.count
         self.cells = params.dims[0] * params.dims[1] * params.dims[2]
         self.ntr = tracers
-        self.h = lib().or_sim_new(C.byref(params), tracers)
+        self.h = self.L.or_sim_new(C.byref(params), tracers)
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().or_sim_free(self.h)
+            self.L.or_sim_free(self.h)
             self.h = None
 
     def set_state(self, pos4=None, vel4=None, prev_vel4=None, prev_p=None, temp=None, ids=None):
         conv = lambda a, k: None if a is None else (f32(a) if k == "f" else u32(a))
         arrs = [conv(pos4, "f"), conv(vel4, "f"), conv(prev_vel4, "f"), conv(prev_p, "f"),
                 conv(temp, "f"), conv(ids, "u")]
-        lib().or_sim_set_state(self.h, *[_ptr(a) for a in arrs])
+        self.L.or_sim_set_state(self.h, *[_ptr(a) for a in arrs])
 
     def state(self):
         n = self.n
         out = dict(pos=np.zeros((n, 4), np.float32), vel=np.zeros((n, 4), np.float32),
                    prev_vel=np.zeros((n, 4), np.float32), prev_p=np.zeros(n, np.float32),
                    temp=np.zeros(n, np.float32), id=np.zeros(n, np.uint32))
-        lib().or_sim_get_state(self.h, *[_ptr(out[k]) for k in
+        self.L.or_sim_get_state(self.h, *[_ptr(out[k]) for k in
                                          ("pos", "vel", "prev_vel", "prev_p", "temp", "id")])
         return out
 
+    def state64(self):
+        n = self.n
+        pos, vel = np.zeros((n, 4), np.float64), np.zeros((n, 4), np.float64)
+        self.L.or_sim_get_state64(self.h, _ptr(pos), _ptr(vel))
+        return dict(pos=pos, vel=vel)
+
     def set_tracers(self, packed):
-        lib().or_sim_set_tracers(self.h, u32(packed).reshape(-1))
+        self.L.or_sim_set_tracers(self.h, u32(packed).reshape(-1))
 
     def tracers(self):
         out = np.zeros(2 * self.ntr, np.uint32)
-        lib().or_sim_get_tracers(self.h, out)
+        self.L.or_sim_get_tracers(self.h, out)
         return out.reshape(-1, 2)
 
     def substep(self, step, div_iters=1, den_iters=5):
-        lib().or_sim_substep(self.h, C.byref(step), div_iters, den_iters)
+        self.L.or_sim_substep(self.h, C.byref(step), div_iters, den_iters)
 
     def substep_tol(self, step, div_tol, den_tol, max_iters=100):
         iters = np.zeros(2, np.uint32)
         res = np.zeros(2, np.float64)
-        lib().or_sim_substep_tol(self.h, C.byref(step), div_tol, den_tol, max_iters, iters, res)
+        self.L.or_sim_substep_tol(self.h, C.byref(step), div_tol, den_tol, max_iters, iters, res)
         return iters, res
 
     def stats(self):
         out = np.zeros(14, np.float32)
-        lib().or_sim_stats(self.h, out)
+        self.L.or_sim_stats(self.h, out)
         return out
 
     def tracer_pass(self, step):
-        lib().or_sim_tracers(self.h, C.byref(step))
+        self.L.or_sim_tracers(self.h, C.byref(step))
 
     def advect(self, step):
-        lib().or_sim_advect(self.h, C.byref(step))
+        self.L.or_sim_advect(self.h, C.byref(step))
 
     def field(self, name):
         n = self.n
@@ -261,7 +288,7 @@ class Sim:
                       wall_grad=((n, 4), np.float32), counters=(2, np.uint32))
         shape, dt = shapes[name]
         out = np.zeros(shape, dt)
-        lib().or_sim_field(self.h, FIELD[name], _ptr(out))
+        self.L.or_sim_field(self.h, FIELD[name], _ptr(out))
         return out
 
 
