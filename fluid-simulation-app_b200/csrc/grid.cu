@@ -13,6 +13,8 @@
 //   k_radix_scatter  stable per-digit scatter: warp match_any ranking in
 //                    input order, per-warp digit counts, tile offsets from
 //                    the look-back scan of the histogram matrix
+#include <string>
+
 #include "grid.cuh"
 
 namespace fcu {
@@ -423,4 +425,57 @@ cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t 
     return cudaGetLastError();
 }
 
+int32_t report_error(int32_t code, const std::string &msg);
+
 }  // namespace fcu
+
+// The look-back scan's bounded wait, run out on purpose: one block of the
+// scan claims tile 1 (the tile counter starts at 1) over a status array in
+// which tile 0 never publishes, so its look-back polls status[0] until the
+// kSpinLimit bound, records ERRF_SCAN_TIMEOUT and treats the missing prefix
+// as zero. Nothing faults or hangs; the context stays usable.
+extern "C" int32_t fluid_selftest_scan_wait(int32_t device, float *ms) {
+    using namespace fcu;
+    auto fail = [](cudaError_t e) {
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_selftest_scan_wait: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e);
+    const uint32_t n = 2 * kScanTile;
+    uint32_t *in = nullptr, *out = nullptr, *err = nullptr;
+    unsigned long long *ctl = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    uint32_t flags = 0;
+    float t = 0.0f;
+    const unsigned long long one = 1ull;
+    do {
+        if ((e = cudaMalloc(&in, 4ull * n)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&out, 4ull * (n + 1))) != cudaSuccess) break;
+        if ((e = cudaMalloc(&ctl, 8ull * 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&err, 4)) != cudaSuccess) break;
+        if ((e = cudaMemset(in, 0, 4ull * n)) != cudaSuccess) break;
+        if ((e = cudaMemset(ctl, 0, 8ull * 4)) != cudaSuccess) break;
+        if ((e = cudaMemset(err, 0, 4)) != cudaSuccess) break;
+        if ((e = cudaMemcpy(ctl, &one, 8, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = cudaEventCreate(&ev[0])) != cudaSuccess) break;
+        if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) break;
+        cudaEventRecord(ev[0]);
+        k_scan_lookback<<<1, kScanThreads>>>(in, out, n, ctl, err, 0, 0);
+        cudaEventRecord(ev[1]);
+        if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) break;
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        if ((e = cudaMemcpy(&flags, err, 4, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+    } while (false);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaFree(in);
+    cudaFree(out);
+    cudaFree(ctl);
+    cudaFree(err);
+    if (e != cudaSuccess) return fail(e);
+    if (ms) *ms = t;
+    if (flags & ERRF_SCAN_TIMEOUT)
+        return report_error(FLUID_ERR_TIMEOUT, "fluid_selftest_scan_wait: the look-back wait gave up, as it should");
+    return FLUID_OK;
+}

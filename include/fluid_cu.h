@@ -464,6 +464,13 @@ int32_t fluid_grid_build_host(const float *pos4, uint32_t n, const FluidGrid *gr
 int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const FluidGrid *grid,
                                 uint32_t *keys, uint32_t *starts, uint32_t *perm, void *stream);
 
+/* Failure detection, exercised (no counterpart in the reference): runs one
+ * block of the grid's look-back scan whose predecessor never publishes, so
+ * the scan's bounded wait (2^20 polls) gives up. Returns FLUID_ERR_TIMEOUT
+ * when the wait gave up and recorded it, as it should; *ms (if not null)
+ * the kernel's time. Nothing faults or hangs, and the device stays usable. */
+int32_t fluid_selftest_scan_wait(int32_t device, float *ms);
+
 #ifdef __cplusplus
 }
 #endif
