@@ -463,30 +463,62 @@ __global__ void __launch_bounds__(256) k_m_gather(uint32_t n, const uint32_t *__
     perm_out[k] = j;
 }
 
-// Walks particle i's list in order, kMB entries at a time: the entries and
-// their gradient scales, then the neighbours' records (load(j)), and only
-// then use(gs, record) for each, so a batch's loads overlap. Same order as
-// a plain loop, so the same sums.
+// Walks this lane's share of particle i's list in order, kMB entries at a
+// time: the entries and their gradient scales, then the neighbours' records
+// (load(j)), and only then use(gs, record) for each, so a batch's loads
+// overlap.
 constexpr int kMB = 4;
 constexpr int kRB = 2;  // the reverse sweeps with wide records
+// Each particle's list is shared by kLanes adjacent lanes of a warp: lane l
+// takes entries l, l + kLanes, ... and the lanes' partial sums are folded by
+// lane_sum (the model fixes its own summation order; at 64k particles one
+// lane per particle leaves most of the GPU's warp slots empty).
+#ifndef ADJ_LANES
+#define ADJ_LANES 4
+#endif
+constexpr int kLanes = ADJ_LANES;
+static_assert(32 % kLanes == 0 && kAdjThreads % kLanes == 0, "lanes of a particle share a warp");
+template <class T>
+DEV T lane_sum(T v) {
+#pragma unroll
+    for (int o = 1; o < kLanes; o <<= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+template <class T>
+DEV V3<T> lane_sum(V3<T> v) {
+    return mk(lane_sum(v.x), lane_sum(v.y), lane_sum(v.z));
+}
+// The particle and lane of a thread of a lane-split sweep; `live` is false
+// for the launch's tail past n, whose lanes take part in the folds with an
+// empty list and write nothing.
+struct LaneOf {
+    uint32_t i, lane;
+    bool live;
+};
+DEV LaneOf lane_of(uint32_t n) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / kLanes;
+    return LaneOf{i < n ? i : n - 1, t % kLanes, i < n};
+}
 template <class T, class R, class Load, class Use>
 DEV void mwalk(const uint32_t *__restrict__ nbr, const T *__restrict__ gsl, uint32_t n, uint32_t i,
-               uint32_t cnt, Load load, Use use) {
-    for (uint32_t k = 0; k < cnt; k += kMB) {
+               uint32_t cnt, uint32_t lane, Load load, Use use) {
+    for (uint32_t k = lane; k < cnt; k += kLanes * kMB) {
         uint32_t j[kMB];
         T g[kMB];
 #pragma unroll
         for (int u = 0; u < kMB; ++u) {
-            const bool ok = k + u < cnt;
-            j[u] = ok ? nbr[(size_t)(k + u) * n + i] : i;
-            g[u] = ok ? gsl[(size_t)(k + u) * n + i] : T(0);
+            const uint32_t kk = k + u * kLanes;
+            const bool ok = kk < cnt;
+            j[u] = ok ? nbr[(size_t)kk * n + i] : i;
+            g[u] = ok ? gsl[(size_t)kk * n + i] : T(0);
         }
         R r[kMB];
 #pragma unroll
         for (int u = 0; u < kMB; ++u) r[u] = load(j[u]);
 #pragma unroll
         for (int u = 0; u < kMB; ++u)
-            if (k + u < cnt) use(g[u], r[u]);
+            if (k + u * kLanes < cnt) use(g[u], r[u]);
     }
 }
 template <class T> struct XV {
@@ -498,19 +530,20 @@ template <class T> struct XK {
 };
 
 // mwalk for the reverse sweeps, which keep no gradient scales: kB entries,
-// then their records, then use(j, record) for each, in list order.
+// then their records, then use(j, record) for each, in the lane's order.
 template <int kB, class R, class Load, class Use>
-DEV void rwalk(const uint32_t *__restrict__ nbr, uint32_t n, uint32_t i, uint32_t cnt, Load load, Use use) {
-    for (uint32_t k = 0; k < cnt; k += kB) {
+DEV void rwalk(const uint32_t *__restrict__ nbr, uint32_t n, uint32_t i, uint32_t cnt, uint32_t lane, Load load,
+               Use use) {
+    for (uint32_t k = lane; k < cnt; k += kLanes * kB) {
         uint32_t j[kB];
 #pragma unroll
-        for (int u = 0; u < kB; ++u) j[u] = k + u < cnt ? nbr[(size_t)(k + u) * n + i] : i;
+        for (int u = 0; u < kB; ++u) j[u] = k + u * kLanes < cnt ? nbr[(size_t)(k + u * kLanes) * n + i] : i;
         R r[kB];
 #pragma unroll
         for (int u = 0; u < kB; ++u) r[u] = load(j[u]);
 #pragma unroll
         for (int u = 0; u < kB; ++u)
-            if (k + u < cnt) use(j[u], r[u]);
+            if (k + u * kLanes < cnt) use(j[u], r[u]);
     }
 }
 template <class T> struct XVK {
@@ -521,42 +554,44 @@ template <class T> struct XVK {
 // d_i = m sum (v_i - v_j).grad W_ij + v_i.wg_i
 template <class T>
 DEV T div_of(const MP<T> &p, uint32_t n, uint32_t i, const V3<T> *__restrict__ x, const V3<T> *__restrict__ v,
-             const uint32_t *__restrict__ nbr, const T *__restrict__ gsl, uint32_t cnt, V3<T> wgi) {
+             const uint32_t *__restrict__ nbr, const T *__restrict__ gsl, uint32_t cnt, V3<T> wgi,
+             uint32_t lane) {
     const V3<T> xi = x[i], vi = v[i];
     T d = T(0);
     mwalk<T, XV<T>>(
-        nbr, gsl, n, i, cnt, [&](uint32_t j) { return XV<T>{x[j], v[j]}; },
+        nbr, gsl, n, i, cnt, lane, [&](uint32_t j) { return XV<T>{x[j], v[j]}; },
         [&](T gs, const XV<T> &q) { d += dot(vi - q.v, gs * (xi - q.x)); });
-    return p.m * d + dot(vi, wgi);
+    return p.m * lane_sum(d) + dot(vi, wgi);
 }
 
 // div_of with each pair's gradient scale recomputed (the reverse sweeps,
 // which keep no scales): the same values, so the same sum.
 template <class T>
 DEV T div_of_radial(const MP<T> &p, uint32_t n, uint32_t i, const V3<T> *__restrict__ x,
-                    const V3<T> *__restrict__ v, const uint32_t *__restrict__ nbr, uint32_t cnt, V3<T> wgi) {
+                    const V3<T> *__restrict__ v, const uint32_t *__restrict__ nbr, uint32_t cnt, V3<T> wgi,
+                    uint32_t lane) {
     const V3<T> xi = x[i], vi = v[i];
     T d = T(0);
     rwalk<kMB, XV<T>>(
-        nbr, n, i, cnt, [&](uint32_t j) { return XV<T>{x[j], v[j]}; },
+        nbr, n, i, cnt, lane, [&](uint32_t j) { return XV<T>{x[j], v[j]}; },
         [&](uint32_t, const XV<T> &q) {
             const V3<T> xij = xi - q.x;
             const Radial<T> R = radial(p, dot(xij, xij));
             d += dot(vi - q.v, R.gs * xij);
         });
-    return p.m * d + dot(vi, wgi);
+    return p.m * lane_sum(d) + dot(vi, wgi);
 }
 
 // sum (kd_i + kd_j) grad W_ij
 template <class T>
 DEV V3<T> kappa_of(uint32_t n, uint32_t i, V3<T> xi, T kdi, const V3<T> *__restrict__ x,
                    const T *__restrict__ kd, const uint32_t *__restrict__ nbr, const T *__restrict__ gsl,
-                   uint32_t cnt) {
+                   uint32_t cnt, uint32_t lane) {
     V3<T> s = zero3<T>();
     mwalk<T, XK<T>>(
-        nbr, gsl, n, i, cnt, [&](uint32_t j) { return XK<T>{x[j], kd[j]}; },
+        nbr, gsl, n, i, cnt, lane, [&](uint32_t j) { return XK<T>{x[j], kd[j]}; },
         [&](T gs, const XK<T> &q) { s = s + (kdi + q.kd) * (gs * (xi - q.x)); });
-    return s;
+    return lane_sum(s);
 }
 
 // Divergence (den = 0) or density (den = 1) prediction; the residual term
@@ -568,10 +603,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_kappa(MP<T> p, uint32_t n, in
                                                          const uint32_t *__restrict__ nbr_n, const T *__restrict__ rho,
                                                          const T *__restrict__ alpha, const V3<T> *__restrict__ wg,
                                                          T *kd, T *pinc, double *res) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     double term = 0.0;
-    if (i < n) {
-        const T d = div_of(p, n, i, x, v, nbr, gsl, nbr_n[i], wg[i]);
+    const T d = div_of(p, n, i, x, v, nbr, gsl, L.live ? nbr_n[i] : 0u, wg[i], L.lane);
+    if (L.live && L.lane == 0) {
         const T r = rho[i], a = alpha[i];
         if (!den) {
             const T dp = d > T(0) ? d : T(0);
@@ -602,11 +638,12 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_apply(MP<T> p, uint32_t n, T 
                                                          const uint32_t *__restrict__ nbr_n, const T *__restrict__ kd,
                                                          const V3<T> *__restrict__ wg, const T *__restrict__ pinc,
                                                          T *pressure) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i];
     const T kdi = kd[i];
-    const V3<T> s = kappa_of(n, i, xi, kdi, x, kd, nbr, gsl, nbr_n[i]);
+    const V3<T> s = kappa_of(n, i, xi, kdi, x, kd, nbr, gsl, L.live ? nbr_n[i] : 0u, L.lane);
+    if (!L.live || L.lane != 0) return;
     const V3<T> dv = p.m * s + kdi * wg[i];
     v_out[i] = v_in[i] - dt * dv;
     if (pinc) pressure[i] += pinc[i];
@@ -621,17 +658,17 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_forces_eval(MP<T> p, uint32_t
                                                                const T *__restrict__ rho, const T *__restrict__ rhon,
                                                                const T *__restrict__ pp, V3<T> *accel, V3<T> *blend,
                                                                T *kd, T *pressure) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i], vi = v[i];
     const T rho_i = rho[i], near_i = rhon[i];
-    const uint32_t cnt = nbr_n[i];
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
     V3<T> visc = zero3<T>(), bl = zero3<T>(), near = zero3<T>(), ten = zero3<T>();
     struct Rec {
         V3<T> x, v;
         T rho, near;
     };
-    rwalk<kRB, Rec>(nbr, n, i, cnt, [&](uint32_t j) { return Rec{x[j], v[j], rho[j], rhon[j]}; },
+    rwalk<kRB, Rec>(nbr, n, i, cnt, L.lane, [&](uint32_t j) { return Rec{x[j], v[j], rho[j], rhon[j]}; },
                     [&](uint32_t, const Rec &q) {
         const V3<T> xij = xi - q.x;
         const T r2 = dot(xij, xij);
@@ -655,6 +692,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_forces_eval(MP<T> p, uint32_t
         const T rt = R.r > T(1e-9f) ? R.r : T(1e-9f);
         ten = ten - (corr * p.m * C / rt) * xij;
     });
+    visc = lane_sum(visc);
+    bl = lane_sum(bl);
+    near = lane_sum(near);
+    ten = lane_sum(ten);
+    if (!L.live || L.lane != 0) return;
     V3<T> ad;
     w_adh<T, T>(p, xi.x, xi.y, xi.z, ad.x, ad.y, ad.z);
     accel[i] = visc + p.k_near * near + p.gamma * ten + (p.beta * p.rho0) * ad;
@@ -674,11 +716,12 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_forces_apply(MP<T> p, uint32_
                                                                 const T *__restrict__ gsl,
                                                                 const uint32_t *__restrict__ nbr_n,
                                                                 const T *__restrict__ kd, const V3<T> *__restrict__ wg) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i];
     const T kdi = kd[i];
-    const V3<T> s = kappa_of(n, i, xi, kdi, x, kd, nbr, gsl, nbr_n[i]);
+    const V3<T> s = kappa_of(n, i, xi, kdi, x, kd, nbr, gsl, L.live ? nbr_n[i] : 0u, L.lane);
+    if (!L.live || L.lane != 0) return;
     const V3<T> forced = v_in[i] + dt * (f + accel[i]) + c * blend[i];
     v_out[i] = forced - dt * (p.m * s + kdi * wg[i]);
 }
@@ -789,16 +832,16 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_apply(MP<T> p, uint32_t n, T 
                                                          const uint32_t *__restrict__ nbr_n, const T *__restrict__ kd,
                                                          const V3<T> *__restrict__ wg, const V3<T> *__restrict__ vbar,
                                                          T *kdbar, V3<T> *xbar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i], vb = vbar[i];
     const T kdi = kd[i];
     const T c = -dt * p.m;
-    const uint32_t cnt = nbr_n[i];
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
     T s = T(0);
     V3<T> xs = zero3<T>();
     rwalk<kMB, XVK<T>>(
-        nbr, n, i, cnt, [&](uint32_t j) { return XVK<T>{x[j], vbar[j], kd[j]}; },
+        nbr, n, i, cnt, L.lane, [&](uint32_t j) { return XVK<T>{x[j], vbar[j], kd[j]}; },
         [&](uint32_t, const XVK<T> &q) {
             const V3<T> xij = xi - q.x;
             const Radial<T> R = radial(p, dot(xij, xij));
@@ -806,6 +849,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_apply(MP<T> p, uint32_t n, T 
             s += dot(R.gs * xij, dvb);
             xs = xs + (c * (kdi + q.k)) * hess(R, xij, dvb);
         });
+    s = lane_sum(s);
+    xs = lane_sum(xs);
+    if (!L.live || L.lane != 0) return;
     const V3<T> wgi = wg[i];
     kdbar[i] = -dt * (p.m * s + dot(wgi, vb));
     const J3<T> J = wall_grad_jac(p, xi);
@@ -825,9 +871,10 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_kappa_a(MP<T> p, uint32_t n, 
                                                            const V3<T> *__restrict__ wg, const T *__restrict__ kdbar,
                                                            const T *__restrict__ pbar, T *dbar, T *rhobar,
                                                            T *alphabar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const T d = div_of_radial(p, n, i, x, v, nbr, nbr_n[i], wg[i]);
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
+    const T d = div_of_radial(p, n, i, x, v, nbr, L.live ? nbr_n[i] : 0u, wg[i], L.lane);
+    if (!L.live || L.lane != 0) return;
     const T r = rho[i], a = alpha[i], kb = kdbar[i];
     T db = T(0), rb = T(0), ab = T(0);
     if (!den) {
@@ -864,14 +911,14 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_kappa_b(MP<T> p, uint32_t n, 
                                                            const uint32_t *__restrict__ nbr_n,
                                                            const V3<T> *__restrict__ wg, const T *__restrict__ dbar,
                                                            V3<T> *vbar, V3<T> *xbar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i], vi = v[i];
     const T di = dbar[i];
-    const uint32_t cnt = nbr_n[i];
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
     V3<T> vs = zero3<T>(), xs = zero3<T>();
     rwalk<kMB, XVK<T>>(
-        nbr, n, i, cnt, [&](uint32_t j) { return XVK<T>{x[j], v[j], dbar[j]}; },
+        nbr, n, i, cnt, L.lane, [&](uint32_t j) { return XVK<T>{x[j], v[j], dbar[j]}; },
         [&](uint32_t, const XVK<T> &q) {
             const T c = p.m * (di + q.k);
             if (c == T(0)) return;
@@ -880,6 +927,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_kappa_b(MP<T> p, uint32_t n, 
             vs = vs + (c * R.gs) * xij;
             xs = xs + c * hess(R, xij, vi - q.v);
         });
+    vs = lane_sum(vs);
+    xs = lane_sum(xs);
+    if (!L.live || L.lane != 0) return;
     vbar[i] = vbar[i] + vs + di * wg[i];
     if (di != T(0)) {
         const J3<T> J = wall_grad_jac(p, xi);
@@ -900,30 +950,33 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_
                                                                 const T *__restrict__ kd, const V3<T> *__restrict__ wg,
                                                                 const V3<T> *__restrict__ vbar, V3<T> *abar, V3<T> *bbar,
                                                                 T *kdbar, V3<T> *xbar, double *fbar, double *cbar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     double red[4] = {0.0, 0.0, 0.0, 0.0};
-    if (i < n) {
-        const V3<T> xi = x[i], vb = vbar[i];
+    const V3<T> xi = x[i], vb = vbar[i];
+    const T kdi = kd[i];
+    const T cc = -dt * p.m;
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
+    T s = T(0);
+    V3<T> xs = zero3<T>();
+    rwalk<kMB, XVK<T>>(
+        nbr, n, i, cnt, L.lane, [&](uint32_t j) { return XVK<T>{x[j], vbar[j], kd[j]}; },
+        [&](uint32_t, const XVK<T> &q) {
+            const V3<T> xij = xi - q.x;
+            const Radial<T> R = radial(p, dot(xij, xij));
+            const V3<T> dvb = vb - q.v;
+            s += dot(R.gs * xij, dvb);
+            xs = xs + (cc * (kdi + q.k)) * hess(R, xij, dvb);
+        });
+    s = lane_sum(s);
+    xs = lane_sum(xs);
+    if (L.live && L.lane == 0) {
         abar[i] = dt * vb;
         bbar[i] = c * vb;
         red[0] = (double)dt * (double)vb.x;
         red[1] = (double)dt * (double)vb.y;
         red[2] = (double)dt * (double)vb.z;
         red[3] = (double)dot(blend[i], vb);
-        const T kdi = kd[i];
-        const T cc = -dt * p.m;
-        const uint32_t cnt = nbr_n[i];
-        T s = T(0);
-        V3<T> xs = zero3<T>();
-        rwalk<kMB, XVK<T>>(
-            nbr, n, i, cnt, [&](uint32_t j) { return XVK<T>{x[j], vbar[j], kd[j]}; },
-            [&](uint32_t, const XVK<T> &q) {
-                const V3<T> xij = xi - q.x;
-                const Radial<T> R = radial(p, dot(xij, xij));
-                const V3<T> dvb = vb - q.v;
-                s += dot(R.gs * xij, dvb);
-                xs = xs + (cc * (kdi + q.k)) * hess(R, xij, dvb);
-            });
         const V3<T> wgi = wg[i];
         kdbar[i] = -dt * (p.m * s + dot(wgi, vb));
         const J3<T> J = wall_grad_jac(p, xi);
@@ -1042,24 +1095,21 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_eval(MP<T> p, uint32_t
                                                                const T *__restrict__ kdbar, const T *__restrict__ pbar,
                                                                V3<T> *xbar, V3<T> *vbar, T *rhobar, T *rhonbar,
                                                                T *ppbar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i], vi = v[i];
     const T rho_i = rho[i], near_i = rhon[i];
     const V3<T> ab = abar[i], bb = bbar[i];
-    // own terms: kd = half / rho^2, pressure = half, half = pp / 2
-    const T kb = kdbar[i];
-    ppbar[i] = T(0.5f) * kb / (rho_i * rho_i) + T(0.5f) * pbar[i];
-    T rb_i = -kb * pp[i] / (rho_i * rho_i * rho_i);
+    T rb_i = T(0);
     T nb_i = T(0);
     V3<T> xs = zero3<T>(), vs = zero3<T>();
-    const uint32_t cnt = nbr_n[i];
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
     struct Rec {
         V3<T> x, v, ab, bb;
         T rho, near;
     };
     rwalk<kRB, Rec>(
-        nbr, n, i, cnt, [&](uint32_t j) { return Rec{x[j], v[j], abar[j], bbar[j], rho[j], rhon[j]}; },
+        nbr, n, i, cnt, L.lane, [&](uint32_t j) { return Rec{x[j], v[j], abar[j], bbar[j], rho[j], rhon[j]}; },
         [&](uint32_t, const Rec &q) {
             const V3<T> xij = xi - q.x;
             const T r2 = dot(xij, xij);
@@ -1072,6 +1122,15 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_eval(MP<T> p, uint32_t
             rb_i += own.rb_a + oth.rb_b;
             nb_i += own.nb + oth.nb;
         });
+    xs = lane_sum(xs);
+    vs = lane_sum(vs);
+    rb_i = lane_sum(rb_i);
+    nb_i = lane_sum(nb_i);
+    if (!L.live || L.lane != 0) return;
+    // own terms: kd = half / rho^2, pressure = half, half = pp / 2
+    const T kb = kdbar[i];
+    ppbar[i] = T(0.5f) * kb / (rho_i * rho_i) + T(0.5f) * pbar[i];
+    rb_i += -kb * pp[i] / (rho_i * rho_i * rho_i);
     const J3<T> Ja = wall_adh_jac(p, xi);
     xs = xs + (p.beta * p.rho0) * jt_mul(Ja, ab);
     xbar[i] = xbar[i] + xs;
@@ -1090,14 +1149,14 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density_a(MP<T> p, uint32_t n
                                                              const T *__restrict__ rho, const T *__restrict__ rhobar,
                                                              const T *__restrict__ alphabar, T *rbt, V3<T> *gbar,
                                                              T *sbar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i];
-    const uint32_t cnt = nbr_n[i];
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
     V3<T> gsum = zero3<T>();
     T gsq = T(0);
     rwalk<kMB, V3<T>>(
-        nbr, n, i, cnt, [&](uint32_t j) { return x[j]; },
+        nbr, n, i, cnt, L.lane, [&](uint32_t j) { return x[j]; },
         [&](uint32_t, const V3<T> &xj) {
             const V3<T> xij = xi - xj;
             const Radial<T> R = radial(p, dot(xij, xij));
@@ -1105,6 +1164,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density_a(MP<T> p, uint32_t n
             gsum = gsum + gw;
             gsq += dot(gw, gw);
         });
+    gsum = lane_sum(gsum);
+    gsq = lane_sum(gsq);
+    if (!L.live || L.lane != 0) return;
     const V3<T> G = p.m * gsum + wall_grad(p, xi);
     const T den = dot(G, G) + p.m * p.m * gsq;
     const T r = rho[i];
@@ -1150,24 +1212,26 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_density_b(MP<T> p, uint32_t n
                                                              const T *__restrict__ rbt, const V3<T> *__restrict__ gbar,
                                                              const T *__restrict__ sbar,
                                                              const T *__restrict__ rhonbar, V3<T> *xbar) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const LaneOf L = lane_of(n);
+    const uint32_t i = L.i;
     const V3<T> xi = x[i];
     const T rb = rbt[i], Sb = sbar[i], nb = rhonbar[i];
     const V3<T> Gb = gbar[i];
-    const uint32_t cnt = nbr_n[i];
+    const uint32_t cnt = L.live ? nbr_n[i] : 0u;
     V3<T> xs = zero3<T>();
     struct Rec {
         V3<T> x, gb;
         T rb, sb, nb;
     };
     rwalk<kRB, Rec>(
-        nbr, n, i, cnt, [&](uint32_t j) { return Rec{x[j], gbar[j], rbt[j], sbar[j], rhonbar[j]}; },
+        nbr, n, i, cnt, L.lane, [&](uint32_t j) { return Rec{x[j], gbar[j], rbt[j], sbar[j], rhonbar[j]}; },
         [&](uint32_t, const Rec &q) {
             const V3<T> xij = xi - q.x;
             const Radial<T> R = radial(p, dot(xij, xij));
             xs = xs + density_pair_bar(p, xij, R, rb, Gb, Sb, nb) - density_pair_bar(p, -xij, R, q.rb, q.gb, q.sb, q.nb);
         });
+    xs = lane_sum(xs);
+    if (!L.live || L.lane != 0) return;
     const J3<T> J = wall_grad_jac(p, xi);
     xs = xs + jt_mul(J, Gb) + (rb * p.rho0) * fill_grad(p, xi);
     xbar[i] = xbar[i] + xs;
@@ -1464,14 +1528,14 @@ struct AdjImpl : AdjBase {
         if (rc != FLUID_OK) return rc;
         k_m_gather<T><<<nblk(n, 256), 256, 0, stream>>>(n, perm, x, v, pp, id, t.x, t.vdiv[0], t.pp, id2, t.perm);
         std::swap(id, id2);
-        const uint32_t B = nblk(n, kAdjThreads);
+        const uint32_t B = nblk(n, kAdjThreads), BL = nblk(n * kLanes, kAdjThreads);
         k_m_density<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, pos4, starts, nullptr, t.nbr, gsl, t.nbr_n,
                                                       t.rho, t.rhon, t.alpha, t.wg, over);
         // divergence loop
         uint32_t nd = decide ? 0u : div_it[k];
         if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
         double *res = decide ? acc : nullptr;
-        k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[0], t.nbr, gsl, t.nbr_n, t.rho, t.alpha,
+        k_m_kappa<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[0], t.nbr, gsl, t.nbr_n, t.rho, t.alpha,
                                                     t.wg, t.kddiv.empty() ? kd : t.kddiv[0], nullptr, res);
         uint32_t it = 0;
         for (;;) {
@@ -1485,20 +1549,20 @@ struct AdjImpl : AdjBase {
                 break;
             }
             T *kd_t = t.kddiv[it];
-            k_m_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vdiv[it], t.vdiv[it + 1], t.nbr, gsl, t.nbr_n,
+            k_m_apply<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vdiv[it], t.vdiv[it + 1], t.nbr, gsl, t.nbr_n,
                                                         kd_t, t.wg, nullptr, nullptr);
             ++it;
             if (decide || it < nd) {
                 if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
-                k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[it], t.nbr, gsl, t.nbr_n, t.rho,
+                k_m_kappa<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[it], t.nbr, gsl, t.nbr_n, t.rho,
                                                             t.alpha, t.wg, t.kddiv[it], nullptr, res);
             }
         }
         nd = it;
         // forces
-        k_m_forces_eval<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.vdiv[nd], t.nbr, t.nbr_n, t.rho, t.rhon,
+        k_m_forces_eval<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, t.x, t.vdiv[nd], t.nbr, t.nbr_n, t.rho, t.rhon,
                                                           t.pp, t.accel, t.blend, t.kdf, pressure);
-        k_m_forces_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, f, c, t.x, t.vdiv[nd], t.vden[0], t.accel,
+        k_m_forces_apply<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, dt, f, c, t.x, t.vdiv[nd], t.vden[0], t.accel,
                                                            t.blend, t.nbr, gsl, t.nbr_n, t.kdf, t.wg);
         // density loop
         const uint32_t ne = decide ? 0u : den_it[k];
@@ -1506,7 +1570,7 @@ struct AdjImpl : AdjBase {
         for (;;) {
             if (!decide && it >= ne) break;
             if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
-            k_m_kappa<T><<<B, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[it], t.nbr, gsl, t.nbr_n, t.rho,
+            k_m_kappa<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[it], t.nbr, gsl, t.nbr_n, t.rho,
                                                         t.alpha, t.wg, t.kdden[it], pinc, res);
             if (decide) {
                 double r;
@@ -1514,7 +1578,7 @@ struct AdjImpl : AdjBase {
                 if (rc != FLUID_OK) return rc;
                 if (!(it < max_iters && r > (double)den_tol)) break;
             }
-            k_m_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vden[it], t.vden[it + 1], t.nbr, gsl, t.nbr_n,
+            k_m_apply<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, dt, t.x, t.vden[it], t.vden[it + 1], t.nbr, gsl, t.nbr_n,
                                                         t.kdden[it], t.wg, pinc, pressure);
             ++it;
         }
@@ -1620,13 +1684,13 @@ struct AdjImpl : AdjBase {
 
     // The density pass reversed: total rho, G and S adjoints, then x.
     void reverse_density(const V3<T> *xs, const uint32_t *nb, const uint32_t *nbn, const T *rho) {
-        const uint32_t B = nblk(n, kAdjThreads);
+        const uint32_t B = nblk(n * kLanes, kAdjThreads);
         k_r_density_a<T><<<B, kAdjThreads, 0, stream>>>(mp, n, xs, nb, nbn, rho, rhobar, alphabar, rbt, gbar, sbar);
         k_r_density_b<T><<<B, kAdjThreads, 0, stream>>>(mp, n, xs, nb, nbn, rbt, gbar, sbar, rhonbar, xbar);
     }
 
     void reverse_substep(uint32_t k, const Tape<T> &t) {
-        const uint32_t B = nblk(n, kAdjThreads), B2 = nblk(n, 256);
+        const uint32_t B = nblk(n * kLanes, kAdjThreads), B2 = nblk(n, 256);
         const uint32_t nd = div_it[k], ne = den_it[k];
         const size_t N = n;
         k_r_integrate<T><<<B2, 256, 0, stream>>>(mp, n, dt, vclamp, t.x, t.vden[ne], t.rho, xbar, vbar);
