@@ -57,7 +57,18 @@ namespace fcu {
 
 namespace {
 
-__device__ __forceinline__ float kernel_q(const DevParams &P, float q) {  // :176-182
+// The kernel's constants a neighbour pair needs, apart from the rest of a
+// box's parameters: a batch's sweeps keep these four in registers and read
+// the others from the box's entry where they are used.
+struct KernelConsts {
+    float sigma, sigma_h, inv_h, support_sq;
+};
+__device__ __forceinline__ KernelConsts kernel_consts(const DevParams &P) {
+    return KernelConsts{P.sigma, P.sigma_h, P.inv_h, P.support_sq};
+}
+
+template <class KP>
+__device__ __forceinline__ float kernel_q(const KP &P, float q) {  // :176-182
     if (q < 1.0f) return P.sigma * (1.0f - 1.5f * q * q * (1.0f - 0.5f * q));
     const float t = 2.0f - q;
     return P.sigma * 0.25f * t * t * t;
@@ -66,7 +77,8 @@ __device__ __forceinline__ float kernel_q(const DevParams &P, float q) {  // :17
 // grad_q (sim_solve.wgsl:184-196) returns (dw / r) * x; this is its scalar
 // dw / r, and 0 under the r < 1e-9 guard (0 * x sums exactly like the
 // guard's zero vector: a signed zero added to any sum leaves it unchanged).
-__device__ __forceinline__ float grad_scale(const DevParams &P, float r, float q) {
+template <class KP>
+__device__ __forceinline__ float grad_scale(const KP &P, float r, float q) {
     if (r < 1e-9f) return 0.0f;
     float dw;
     if (q < 1.0f) {
@@ -342,6 +354,13 @@ __device__ __forceinline__ DevParams params_of(const Geo &g, uint32_t bi) {
     if (kB) return g.box[bi];
     return g.one;
 }
+// The same by reference: the box's entry in global memory (batch), or the
+// kernel's own parameter space (one box: the kernel takes Geo as
+// __grid_constant__, so no copy is made).
+template <bool kB>
+__device__ __forceinline__ const DevParams &params_ref(const Geo &g, uint32_t bi) {
+    return kB ? g.box[bi] : g.one;
+}
 template <bool kB>
 __device__ __forceinline__ uint32_t cell_base_of(const Geo &g, uint32_t bi) {
     return kB ? __ldg(&g.cell_base[bi]) : 0u;
@@ -413,7 +432,8 @@ struct DensitySums {
     F3 grad_sum;
 };
 
-__device__ __forceinline__ float density_pair(const DevParams &P, DensitySums &d, F3 pos, F3 vel,
+template <class KP>
+__device__ __forceinline__ float density_pair(const KP &P, DensitySums &d, F3 pos, F3 vel,
                                               F3 x, float r2, float4 vj) {
     const float r = sqrtf(r2);
     const float q = r * P.inv_h;
@@ -469,7 +489,8 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
 }
 
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_density_div(Geo g, SimBufs b, int slot) {
+__global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB)
+    k_density_div(const __grid_constant__ Geo g, SimBufs b, int slot) {
     __shared__ uint16_t s_hit[kStage + FCU_DD_CHUNK - 1][TPB];
     __shared__ uint32_t s_beg[9][TPB];
     __shared__ uint32_t s_end[9][TPB];
@@ -480,7 +501,8 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
     if (live) {
-        const DevParams P = params_of<kB>(g, bi);
+        const DevParams &P = params_ref<kB>(g, bi);
+        const KernelConsts K = kernel_consts(P);
         const uint32_t base = cell_base_of<kB>(g, bi);
         const float dt = g.st[bi].s.dt;
         const F3 pos = xyz(__ldg(&b.wpos[i]));
@@ -539,7 +561,7 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
 #pragma unroll
                         for (int u = 0; u < FCU_DD_CHUNK; ++u) {
                             const uint32_t ku = k + u;
-                            if (ku < e && ku != i && r2[u] < P.support_sq) {
+                            if (ku < e && ku != i && r2[u] < K.support_sq) {
                                 s_hit[staged][tid] = (uint16_t)((r << 12) | (ku - rs));
                                 ++staged;
                             }
@@ -549,7 +571,7 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
 #else
                     if (k != i) {
                         const F3 x = pos - xyz(__ldg(&b.wpos[k]));
-                        if (dot(x, x) < P.support_sq) {
+                        if (dot(x, x) < K.support_sq) {
                             s_hit[staged][tid] = (uint16_t)((r << 12) | (k - rs));
                             ++staged;
                         }
@@ -576,7 +598,7 @@ __global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB) k_densi
                     for (int u = 0; u < kP2; ++u) {
                         if (h + u < staged) {
                             const F3 x = pos - xyz(pj[u]);
-                            const float gs = density_pair(P, d, pos, vel, x, dot(x, x), vj[u]);
+                            const float gs = density_pair(K, d, pos, vel, x, dot(x, x), vj[u]);
                             const uint32_t idx = found + h + u;
                             if (idx < cap) b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
                         }
