@@ -1066,18 +1066,39 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats_partial(Geo g, SimBufs 
 }
 
 template <bool kB>
-__global__ void k_stats_final(Geo g, SimBufs b, uint32_t chunks) {
-    const uint32_t bi = blockIdx.x * blockDim.x + threadIdx.x;
-    if (bi >= g.nboxes) return;
+__global__ void __launch_bounds__(kStatsThreads) k_stats_final(Geo g, SimBufs b, uint32_t chunks) {
+    // one block per box: thread t folds chunks t, t + blockDim, ..., then the
+    // warps and the block fold the threads (min and max are exact in any order)
+    const uint32_t bi = blockIdx.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ float s_w[kStatsThreads / 32][11];
     const bool is_max[11] = {true, false, true, false, true, false, true, false, true, false, true};
     const float *part = b.stats_part + (size_t)bi * chunks * 12;
     float out[11];
-    for (int q = 0; q < 11; ++q) out[q] = part[q];
-    for (uint32_t k = 1; k < chunks; ++k)
+    const uint32_t k0 = threadIdx.x < chunks ? threadIdx.x : 0u;
+#pragma unroll
+    for (int q = 0; q < 11; ++q) out[q] = part[k0 * 12 + q];
+    for (uint32_t k = threadIdx.x + blockDim.x; k < chunks; k += blockDim.x)
+#pragma unroll
         for (int q = 0; q < 11; ++q) {
             const float v = part[k * 12 + q];
             out[q] = is_max[q] ? fmaxf(out[q], v) : fminf(out[q], v);
         }
+#pragma unroll
+    for (int q = 0; q < 11; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const float v = __shfl_xor_sync(0xffffffffu, out[q], o);
+            out[q] = is_max[q] ? fmaxf(out[q], v) : fminf(out[q], v);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 11; ++q) s_w[warp][q] = out[q];
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (uint32_t w = 1; w < blockDim.x / 32; ++w)
+#pragma unroll
+        for (int q = 0; q < 11; ++q) out[q] = is_max[q] ? fmaxf(out[q], s_w[w][q]) : fminf(out[q], s_w[w][q]);
     float *s = b.stats + (size_t)bi * 16;
     s[0] = (float)((double)b.stats_acc[bi] / kFixedScale / (double)params_of<kB>(g, bi).count);
     b.stats_acc[bi] = 0ull;
@@ -1280,13 +1301,12 @@ void launch_tol_finish(cudaStream_t s, const Geo &g, int which, int first, float
 void launch_stats(cudaStream_t s, const Geo &g, const SimBufs &b, uint32_t chunks) {
     if (!g.nboxes || !chunks) return;
     const dim3 grid(chunks, g.nboxes);
-    const uint32_t fb = blocks_for(g.nboxes, 128);
     if (g.box_of) {
         k_stats_partial<true><<<grid, kStatsThreads, 0, s>>>(g, b);
-        k_stats_final<true><<<fb, 128, 0, s>>>(g, b, chunks);
+        k_stats_final<true><<<g.nboxes, kStatsThreads, 0, s>>>(g, b, chunks);
     } else {
         k_stats_partial<false><<<grid, kStatsThreads, 0, s>>>(g, b);
-        k_stats_final<false><<<fb, 128, 0, s>>>(g, b, chunks);
+        k_stats_final<false><<<g.nboxes, kStatsThreads, 0, s>>>(g, b, chunks);
     }
 }
 void launch_splat(cudaStream_t s, const DevParams &P, const SimBufs &b) {

@@ -75,7 +75,7 @@ struct Geo {
 };
 
 constexpr int kSolveThreads = 128;
-constexpr int kStatsChunks = 148;
+constexpr int kStatsChunks = 592;  // 4 blocks of kStatsThreads per SM at 1M particles
 constexpr int kStatsThreads = 256;
 
 // A tolerance loop's gate: the kernel skips boxes whose loop has stopped.
