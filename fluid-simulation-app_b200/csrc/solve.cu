@@ -1128,19 +1128,37 @@ __device__ __forceinline__ int32_t to_fixed(float v) {  // i32(v * 65536): satur
     return __float2int_rz(v * 65536.0f);
 }
 
+// The lanes of a warp whose particles share a cell add their fixed-point
+// velocities first (__reduce_add_sync over the match_any group: wrapping
+// 32-bit sums, like the atomics, so the cell totals are the same bits) and
+// one lane adds the group's total: slots are in cell order, so a warp's
+// particles sit in a few cells.
 __global__ void __launch_bounds__(256) k_splat(DevParams P, SimBufs b) {  // :98-114
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.count) return;
-    const float4 p = __ldg(&b.pos[i]);
-    const uint32_t cx = axis_cell(p.x, P.box_min[0], P.cell, P.dims[0]);
-    const uint32_t cy = axis_cell(p.y, P.box_min[1], P.cell, P.dims[1]);
-    const uint32_t cz = axis_cell(p.z, P.box_min[2], P.cell, P.dims[2]);
-    const uint32_t c = ((cz * P.dims[1] + cy) * P.dims[0] + cx) * 4u;
-    const float4 v = __ldg(&b.vel[i]);
-    atomicAdd(&b.vel_grid[c], to_fixed(v.x));
-    atomicAdd(&b.vel_grid[c + 1], to_fixed(v.y));
-    atomicAdd(&b.vel_grid[c + 2], to_fixed(v.z));
-    atomicAdd(&b.vel_grid[c + 3], 1);
+    const bool live = i < P.count;
+    uint32_t c = 0xffffffffu;
+    uint32_t fx = 0, fy = 0, fz = 0;
+    if (live) {
+        const float4 p = __ldg(&b.pos[i]);
+        const uint32_t cx = axis_cell(p.x, P.box_min[0], P.cell, P.dims[0]);
+        const uint32_t cy = axis_cell(p.y, P.box_min[1], P.cell, P.dims[1]);
+        const uint32_t cz = axis_cell(p.z, P.box_min[2], P.cell, P.dims[2]);
+        c = ((cz * P.dims[1] + cy) * P.dims[0] + cx) * 4u;
+        const float4 v = __ldg(&b.vel[i]);
+        fx = (uint32_t)to_fixed(v.x);
+        fy = (uint32_t)to_fixed(v.y);
+        fz = (uint32_t)to_fixed(v.z);
+    }
+    const uint32_t peers = __match_any_sync(0xffffffffu, c);
+    fx = __reduce_add_sync(peers, fx);
+    fy = __reduce_add_sync(peers, fy);
+    fz = __reduce_add_sync(peers, fz);
+    if (live && (threadIdx.x & 31u) == (uint32_t)(__ffs(peers) - 1)) {
+        atomicAdd(&b.vel_grid[c], (int32_t)fx);
+        atomicAdd(&b.vel_grid[c + 1], (int32_t)fy);
+        atomicAdd(&b.vel_grid[c + 2], (int32_t)fz);
+        atomicAdd(&b.vel_grid[c + 3], __popc(peers));
+    }
 }
 
 __global__ void __launch_bounds__(256) k_resolve(SimBufs b, uint32_t cells) {  // :122-138
