@@ -998,7 +998,7 @@ __global__ void __launch_bounds__(256) k_tol_finish(Geo g, int which, int first,
 
 // ---- reduce_stats (sim_solve.wgsl:800-874) ---------------------------------
 // Per box, per-chunk partials (block (chunk, box) strides through the box's
-// slots), then one thread per box folds them; min and max are exact in any
+// slots), then one block per box folds them; min and max are exact in any
 // order and the compression sum is an integer sum.
 template <bool kB>
 __global__ void __launch_bounds__(kStatsThreads) k_stats_partial(Geo g, SimBufs b) {
