@@ -735,7 +735,14 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
     if (live && !(kDiv && gated_out<kB>(g, bi, gate))) {
-    const DevParams P = params_of<kB>(g, bi);
+    // a batch reads its box's constants from the box's entry where they are
+    // used, keeping the pair loop's few in registers; one box copies them
+    // from parameter space as before
+    DevParams Pc;
+    if (!kB) Pc = g.one;
+    const DevParams &P = kB ? g.box[bi] : Pc;
+    const KernelConsts K = kernel_consts(P);
+    const float mass = P.mass, inv_h = P.inv_h, rho0 = P.rho0, soft = 0.01f * P.h * P.h;
     const float coh_c = 2.0f * P.h;
     const float c3 = coh_c * coh_c * coh_c;
     const float coh_k = 32.0f / (3.14159265f * c3 * c3 * c3);
@@ -769,18 +776,18 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
         const float r2 = dot(x, x);
         const float r = sqrtf(r2);
         const float rho_j = q.rho;
-        const float f = dot(x, e) / (r2 + 0.01f * P.h * P.h);
-        const float pair = P.mass / (rho_i * rho_j) * f;
+        const float f = dot(x, e) / (r2 + soft);
+        const float pair = mass / (rho_i * rho_j) * f;
         const F3 dv = vel - xyz(q.v);
         if (kDiv) drho += dot(dv, e);
-        const float wn = fmaxf(1.0f - r * P.inv_h, 0.0f);
+        const float wn = fmaxf(1.0f - r * inv_h, 0.0f);
         near = near + ((near_i + q.near) * wn * wn) * (x / fmaxf(r, 1e-5f));
         visc = visc + (visc_k * pair) * dv;
-        blend = blend - (P.mass / rho_j * kernel_q(P, r * P.inv_h)) * dv;
+        blend = blend - (mass / rho_j * kernel_q(K, r * inv_h)) * dv;
         heat += heat_k * pair * (temp - q.temp);
         heat -= diss_k * pair * dot(dv, dv);
-        const float corr = 2.0f * P.rho0 / (rho_i + rho_j);
-        tension = tension - ((corr * P.mass * cohesion(r, coh_c, coh_k, coh_near)) * x) / fmaxf(r, 1e-9f);
+        const float corr = 2.0f * rho0 / (rho_i + rho_j);
+        tension = tension - ((corr * mass * cohesion(r, coh_c, coh_k, coh_near)) * x) / fmaxf(r, 1e-9f);
     });
     const F3 adh = (beta * P.rho0) * wall_adh_sum(P, pos);
     const F3 acc = visc + K_NEAR * near + gamma * tension + adh;
