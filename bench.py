@@ -29,6 +29,9 @@ their own streams at once), for the batch-over-plain ratio.
 adjoint: the adjoint workload (65,536 particles, 120 frames): one forward
 and one backward of the differentiable model, timed on the device, next to
 the production step on the same configuration.
+
+grid: the grid build alone on 16,777,216 positions in 2^24 cells, in three
+distributions, timed on the device, against its algorithmic bytes.
 """
 import argparse
 import ctypes as C
@@ -82,6 +85,31 @@ def peaks():
             p = json.load(f)
         return float(p["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def copy_gbs(device):
+    """STREAM-style copy on this GPU, measured beside the kernels it judges:
+    bytes read + written per second (GB/s) over ten 2 GiB device-to-device
+    copies, after three untimed ones, CUDA events on the current stream."""
+    import torch
+
+    src = torch.ones(1 << 29, dtype=torch.float32, device=device)
+    dst = torch.empty_like(src)
+    for _ in range(3):
+        dst.copy_(src)
+    torch.cuda.synchronize(device)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 10
+    e0.record()
+    for _ in range(reps):
+        dst.copy_(src)
+    e1.record()
+    e1.synchronize()
+    gbs = 2.0 * src.numel() * src.element_size() * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+    del src, dst
+    torch.cuda.empty_cache()
+    return gbs
 
 
 class Clocks:
@@ -209,14 +237,14 @@ def cuda_arm(args):
     value = n * all_substeps / (ms_max / 1000.0)
 
     # kernel launches inside the timed region: per substep the grid build
-    # (keys, scan, 3 per digit pass), gather, density_div and its residual
+    # (keys, one per digit pass, starts scan), gather, density_div and its residual
     # step, forces pair, first density prediction and its residual step,
     # integrate; 3 per loop iteration; per frame stats (2) and tracers (3).
     passes = 1
     cells = sim.cells
     while (cells - 1) >> (8 * passes):
         passes += 1
-    fixed = 2 + 3 * passes + 1 + 2 + 4 + 1
+    fixed = 2 + passes + 1 + 2 + 4 + 1
     launches = fixed * substeps + 3 * (div_it + den_it) + 5 * args.steps
 
     # e2e: a fresh replica, frames through the C ABI with a stats read back
@@ -276,6 +304,7 @@ def cuda_arm(args):
     avg_ms = mean[dom]
     achieved = ALGO_BYTES[dom] * n / (avg_ms / 1000.0) / 1e9
     peak, peak_kind = peaks()
+    copy_peak = copy_gbs(local)
     traffic = NCU_TRAFFIC_PER_PARTICLE.get(dom)
 
     # the CPU oracle on this host over one substep of the same state
@@ -291,6 +320,7 @@ def cuda_arm(args):
     sim.close()
     batched = None if args.no_batched else batched_leg(args, fcu, wl, world, rank, local, value / world)
     adjoint = None if args.no_adjoint else adjoint_leg(args, fcu, wl, world, local)
+    grid = None if args.no_grid else grid_leg(fcu, wl, local, peak, copy_peak)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -322,6 +352,8 @@ def cuda_arm(args):
                          "mean_neighbours": mean_nbrs,
                          "achieved_with_list": (ALGO_BYTES[dom] + list_bytes) * n / (avg_ms / 1000.0) / 1e9,
                          "frac_with_list": (ALGO_BYTES[dom] + list_bytes) * n / (avg_ms / 1000.0) / 1e9 / peak,
+                         "copy_gbs_measured_here": copy_peak,
+                         "frac_of_copy_measured_here": achieved / copy_peak,
                          "kernel_ms": mean,
                          "ms_per_substep_by_kernel": share},
             "cpu_baseline": cpu,
@@ -329,6 +361,7 @@ def cuda_arm(args):
             "gpu_launches": launches,
             "batched": batched,
             "adjoint": adjoint,
+            "grid": grid,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -455,6 +488,63 @@ def plain_boxes_leg(fcu, cfgs, steps, nw, batch_value):
 
 ADJ_FRAMES = 120
 ADJ_CHECKPOINT = 10
+
+
+GRID_SIDE = 256
+GRID_BUILDS = 10
+
+
+def grid_leg(fcu, wl, local, peak, copy_peak):
+    """The grid workload: 16,777,216 positions in a 256^3-cell box (cell 1),
+    in the three seeded distributions (uniform; 90 % packed into the lowest
+    tenth; eight Gaussian clusters of sigma 4 cells), each built into
+    starts[C+1] and the stable permutation by fluid_grid_build. Three
+    untimed builds, then ten timed on the device with CUDA events. The
+    positions (268 MB) exceed L2, so no flush. Algorithmic bytes per build:
+    positions 16 + key 4 + 4 (written, read back) + permutation 4 per
+    position, 8 per cell for the counts and starts."""
+    import torch
+    dev = torch.device("cuda", local)
+    n, side = 1 << 24, GRID_SIDE
+    cells = side ** 3
+    g = fcu.FluidGrid()
+    g.min[:] = [0.0, 0.0, 0.0]
+    g.cell = 1.0
+    g.dims[:] = [side, side, side]
+    ws_bytes = fcu.grid_workspace_bytes(n, g)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    starts = torch.empty(cells + 1, dtype=torch.int32, device=dev)
+    perm = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    algo = 36.0 * n + 8.0 * cells
+    out = {"workload": "grid_16m", "positions": n, "cells": cells,
+           "algorithmic_bytes_per_build": algo, "builds_timed": GRID_BUILDS}
+    for kind, seed in (("uniform", 1), ("packed", 2), ("gaussian", 3)):
+        pos = torch.from_numpy(wl.grid_positions(kind, n, side, seed)).to(dev)
+
+        def build():
+            fcu.grid_build_device(pos.data_ptr(), n, g, 0, starts.data_ptr(), perm.data_ptr(),
+                                  ws.data_ptr(), ws_bytes, stream.cuda_stream)
+
+        for _ in range(3):
+            build()
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(GRID_BUILDS):
+            build()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / GRID_BUILDS
+        gbs = algo / (ms / 1e3) / 1e9
+        out[kind] = {"ms_per_build": ms, "positions_per_s": n / (ms / 1e3),
+                     "achieved_gbs": gbs, "frac": gbs / peak,
+                     "frac_of_copy_measured_here": gbs / copy_peak}
+        del pos
+    del ws, starts, perm
+    torch.cuda.empty_cache()
+    return out
 
 
 def adjoint_leg(args, fcu, wl, world, local):
@@ -625,14 +715,23 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="time the device loop only (profiling runs)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-boxes leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
+    ap.add_argument("--no-grid", action="store_true", help="skip the 16.7M-position grid leg")
     ap.add_argument("--no-plain-boxes", action="store_true",
                     help="skip stepping the batched boxes as separate plain sims")
     ap.add_argument("--profile-substeps", type=int, default=0,
                     help="after the warm-up, run this many substeps as direct launches timed per kernel, then exit")
+    ap.add_argument("--grid-only", action="store_true",
+                    help="run the 16.7M-position grid leg alone and print it (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
-    if args.impl == "reference":
+    if args.grid_only:
+        import torch
+        torch.cuda.set_device(0)
+        fcu = load("fluidcu", os.path.join(PKG, "fluidcu.py"))
+        wl = load("workloads", os.path.join(PKG, "workloads.py"))
+        print(json.dumps(grid_leg(fcu, wl, 0, peaks()[0], copy_gbs(0))), flush=True)
+    elif args.impl == "reference":
         reference_arm(args)
     else:
         cuda_arm(args)

@@ -1495,7 +1495,7 @@ struct AdjImpl : AdjBase {
         }
         g.cell = P.cell;
         AK(cudaMemsetAsync(gw.err, 0, 4, stream));
-        AK(grid_build_enqueue(stream, pos4, n, g, keys, starts, perm, gw, false, nullptr, nullptr, nullptr, 1));
+        AK(grid_build_enqueue(stream, pos4, n, g, keys, starts, perm, gw, nullptr, nullptr, nullptr, 1));
         return FLUID_OK;
     }
 

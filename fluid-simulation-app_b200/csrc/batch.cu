@@ -122,7 +122,7 @@ cudaError_t batch_enqueue(FluidBatch *s, cudaStream_t st, uint32_t div_iters, ui
     k_clear_acc<<<s->nboxes, 128, 0, st>>>(s->solve);
     const BoxKeys bk = s->keys();
     cudaError_t e = grid_build_enqueue(st, s->b.pos, s->n, GridGeom{}, s->b.keys, s->b.starts, s->b.perm,
-                                       s->gw, true, s->ring, s->cur, s->solve, kBatchRing, &bk);
+                                       s->gw, s->ring, s->cur, s->solve, kBatchRing, &bk);
     if (e != cudaSuccess) return e;
     const Geo g = s->geo();
     launch_gather(st, s->b, s->n);
@@ -186,7 +186,7 @@ int32_t batch_graph_tolerance(FluidBatch *s, cudaGraphExec_t *out) {
     k_clear_acc<<<s->nboxes, 128, 0, st>>>(s->solve);
     const BoxKeys bk = s->keys();
     cudaError_t e = grid_build_enqueue(st, s->b.pos, s->n, GridGeom{}, s->b.keys, s->b.starts, s->b.perm,
-                                       s->gw, true, s->ring, s->cur, s->solve, kBatchRing, &bk);
+                                       s->gw, s->ring, s->cur, s->solve, kBatchRing, &bk);
     const Geo geo = s->geo();
     // forces_eval after every divergence apply, forming the prediction that
     // decides the loop (as the one-box tolerance substep)
@@ -380,7 +380,6 @@ int32_t batch_create_into(FluidBatch *s, const FluidSimConfig *boxes, uint32_t n
     BK(cudaMemcpy(s->d_cell_base, s->cell_base.data(), 4 * nb, cudaMemcpyHostToDevice));
     BK(cudaMemcpy(s->d_first, s->first.data(), 4 * nb, cudaMemcpyHostToDevice));
     BK(cudaMemset(s->solve, 0, nb * sizeof(DevSolve)));
-    BK(cudaMemset(s->gw.counts, 0, 4 * C));
     BK(cudaDeviceSynchronize());
     cudaGraphExec_t g;
     return batch_graph(s, &g);
@@ -574,7 +573,7 @@ int32_t timed_substep(FluidBatch *s, int tpb, float *ms, cudaEvent_t *ev) {
     for (int k = 0; k < kTuneCount; ++k) g.tpb[k] = (uint16_t)tpb;
     k_clear_acc<<<s->nboxes, 128, 0, st>>>(s->solve);
     const BoxKeys bk = s->keys();
-    BK(grid_build_enqueue(st, s->b.pos, s->n, GridGeom{}, s->b.keys, s->b.starts, s->b.perm, s->gw, true,
+    BK(grid_build_enqueue(st, s->b.pos, s->n, GridGeom{}, s->b.keys, s->b.starts, s->b.perm, s->gw,
                           nullptr, nullptr, s->solve, kBatchRing, &bk));
     launch_gather(st, s->b, s->n);
     int e = 0;

@@ -6,13 +6,19 @@
 // a cell by atomic arrival; this build is stable (ascending input index inside
 // a cell), the order a sequential counting sort produces.
 //
-//   k_cell_keys      key = cell_of(pos), warp-aggregated histogram
-//   k_scan_lookback  single-pass exclusive scan, decoupled look-back with
-//                    warp shuffles and ballots; every spin is bounded
-//   k_radix_hist     per-tile digit histograms (bin-major matrix)
-//   k_radix_scatter  stable per-digit scatter: warp match_any ranking in
-//                    input order, per-warp digit counts, tile offsets from
-//                    the look-back scan of the histogram matrix
+//   k_cell_keys      key = cell_of(pos), and every radix pass's digit
+//                    counts over all keys
+//   k_radix_pass     one stable 8-bit digit pass: warp ranking in input
+//                    order (digit peers from eight ballots), each tile's
+//                    digit offsets by decoupled look-back over the earlier
+//                    tiles, the tile staged in shared memory in digit order
+//                    and written out coalesced; the last pass also stores
+//                    the end of every run of equal keys at starts[key + 1]
+//   k_scan_lookback  single-pass scan (sum or max), decoupled look-back with
+//                    warp shuffles and ballots; every spin is bounded. The
+//                    inclusive max-scan of the run ends gives starts, the
+//                    exclusive scan of the cell counts, without counting
+#include <algorithm>
 #include <string>
 
 #include "grid.cuh"
@@ -32,90 +38,149 @@ __device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long lon
 __device__ __forceinline__ void st_relaxed(unsigned long long *p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
-__device__ __forceinline__ uint32_t warp_sum_u32(uint32_t v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
 }
 
-// Cell key of every position, and the cell histogram. Block 0 also moves
-// the substep's Step block from the ring into `cur` for the kernels after it.
-__global__ void __launch_bounds__(256) k_cell_keys(const float4 *__restrict__ pos, uint32_t n,
-                                                   GridGeom g, uint32_t *__restrict__ keys,
-                                                   uint32_t *__restrict__ counts,
-                                                   const DevStep *__restrict__ ring, DevStep *cur,
-                                                   DevSolve *solve, uint32_t ring_size) {
+// The lanes of `act` whose 8-bit digit equals this lane's: what
+// __match_any_sync(act, d) returns, from one ballot per digit bit (cheaper
+// than the general match on sm_100). Every lane of the warp calls it.
+__device__ __forceinline__ uint32_t digit_peers(uint32_t act, uint32_t d) {
+    uint32_t m = act;
+#pragma unroll
+    for (int b = 0; b < kRadixBits; ++b) {
+        const uint32_t bit = (d >> b) & 1u;
+        const uint32_t bal = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? bal : ~bal;
+    }
+    return m;
+}
+
+// Adds the run of equal digits this lane starts (in adjacent lanes) to the
+// shared histogram h; positions in cell order give long runs. Every lane of
+// the warp calls it.
+__device__ __forceinline__ void count_digit_runs(uint32_t *h, bool live, uint32_t d) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t live_mask = __ballot_sync(0xffffffffu, live);
+    const uint32_t prev = __shfl_up_sync(0xffffffffu, d, 1);
+    const bool prev_live = lane > 0 && ((live_mask >> (lane - 1)) & 1u);
+    const bool head = live && (!prev_live || prev != d);
+    const uint32_t stops = __ballot_sync(0xffffffffu, head) | ~live_mask;
+    if (head) {
+        const uint32_t after = stops & ~((2u << lane) - 1u);  // stops above this lane
+        const uint32_t end = after ? (uint32_t)(__ffs(after) - 1) : 32u;
+        atomicAdd(&h[d], end - lane);
+    }
+}
+
+// Every pass's digit counts over all keys: a block's shared histograms,
+// then one global add per nonzero bin. Every lane of the block calls both.
+__device__ __forceinline__ void count_digits(uint32_t (*h)[kRadix], int passes, bool live, uint32_t key) {
+    for (int p = 0; p < passes; ++p) count_digit_runs(h[p], live, (key >> (p * kRadixBits)) & (kRadix - 1));
+}
+__device__ __forceinline__ void flush_digits(uint32_t (*h)[kRadix], int passes, uint32_t *digit_counts) {
+    __syncthreads();
+    for (int p = 0; p < passes; ++p) {
+        const uint32_t c = h[p][threadIdx.x];
+        if (c) atomicAdd(&digit_counts[p * kRadix + threadIdx.x], c);
+    }
+}
+
+// Cell key of every position, and every radix pass's digit counts. A
+// grid-stride loop over a capped grid, so the digit counts leave each block
+// once. Block 0 also moves the substep's Step block from the ring into
+// `cur` for the kernels after it.
+__global__ void __launch_bounds__(kSortThreads) k_cell_keys(const float4 *__restrict__ pos, uint32_t n,
+                                                            GridGeom g, uint32_t *__restrict__ keys,
+                                                            int passes, uint32_t *digit_counts,
+                                                            const DevStep *__restrict__ ring, DevStep *cur,
+                                                            DevSolve *solve, uint32_t ring_size) {
+    __shared__ uint32_t h[kMaxPasses][kRadix];
     if (ring && blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t c = solve->cursor;
         *cur = ring[c % ring_size];
         solve->cursor = c + 1u;
     }
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
-    uint32_t key = 0;
-    if (live) {
-        const float4 p = __ldg(&pos[i]);
-        const uint32_t cx = axis_cell(p.x, g.min[0], g.cell, g.dims[0]);
-        const uint32_t cy = axis_cell(p.y, g.min[1], g.cell, g.dims[1]);
-        const uint32_t cz = axis_cell(p.z, g.min[2], g.cell, g.dims[2]);
-        key = (cz * g.dims[1] + cy) * g.dims[0] + cx;
-        keys[i] = key;
+    for (int p = 0; p < kMaxPasses; ++p) h[p][threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t at = (uint64_t)blockIdx.x * kSortThreads; at < n; at += (uint64_t)gridDim.x * kSortThreads) {
+        const uint64_t i = at + threadIdx.x;
+        const bool live = i < n;
+        uint32_t key = 0;
+        if (live) {
+            const float4 p = __ldg(&pos[i]);
+            const uint32_t cx = axis_cell(p.x, g.min[0], g.cell, g.dims[0]);
+            const uint32_t cy = axis_cell(p.y, g.min[1], g.cell, g.dims[1]);
+            const uint32_t cz = axis_cell(p.z, g.min[2], g.cell, g.dims[2]);
+            key = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+            keys[i] = key;
+        }
+        count_digits(h, passes, live, key);
     }
-    const uint32_t act = __ballot_sync(0xffffffffu, live);
-    if (live) {
-        const uint32_t peers = __match_any_sync(act, key);
-        if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&counts[key], __popc(peers));
-    }
+    flush_digits(h, passes, digit_counts);
 }
 
 // The same over a batch of boxes: box b's key is cell_base[b] plus its
 // cell in its own grid. Block 0 moves the substep's nboxes Step blocks
 // (ring entry `cursor`, box-major) into cur[0 .. nboxes-1].
-__global__ void __launch_bounds__(256) k_box_keys(const float4 *__restrict__ pos, uint32_t n,
-                                                  BoxKeys bk, uint32_t *__restrict__ keys,
-                                                  uint32_t *__restrict__ counts,
-                                                  const DevStep *__restrict__ ring, DevStep *cur,
-                                                  DevSolve *solve, uint32_t ring_size) {
+__global__ void __launch_bounds__(kSortThreads) k_box_keys(const float4 *__restrict__ pos, uint32_t n,
+                                                           BoxKeys bk, uint32_t *__restrict__ keys,
+                                                           int passes, uint32_t *digit_counts,
+                                                           const DevStep *__restrict__ ring, DevStep *cur,
+                                                           DevSolve *solve, uint32_t ring_size) {
+    __shared__ uint32_t h[kMaxPasses][kRadix];
     if (ring && blockIdx.x == 0) {
         const uint32_t c = solve->cursor;
         const DevStep *src = ring + (size_t)(c % ring_size) * bk.nboxes;
         for (uint32_t b = threadIdx.x; b < bk.nboxes; b += blockDim.x) cur[b] = src[b];
-        __syncthreads();
+        __syncthreads();  // every thread has read the cursor before it moves
         if (threadIdx.x == 0) solve->cursor = c + 1u;
     }
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
-    uint32_t key = 0;
-    if (live) {
-        const uint32_t b = __ldg(&bk.box_of[i]);
-        const DevParams *P = &bk.box[b];
-        const float4 p = __ldg(&pos[i]);
-        const float cell = __ldg(&P->cell);
-        const uint32_t dx = __ldg(&P->dims[0]), dy = __ldg(&P->dims[1]), dz = __ldg(&P->dims[2]);
-        const uint32_t cx = axis_cell(p.x, __ldg(&P->box_min[0]), cell, dx);
-        const uint32_t cy = axis_cell(p.y, __ldg(&P->box_min[1]), cell, dy);
-        const uint32_t cz = axis_cell(p.z, __ldg(&P->box_min[2]), cell, dz);
-        key = __ldg(&bk.cell_base[b]) + (cz * dy + cy) * dx + cx;
-        keys[i] = key;
+    for (int p = 0; p < kMaxPasses; ++p) h[p][threadIdx.x] = 0;
+    __syncthreads();
+    for (uint64_t at = (uint64_t)blockIdx.x * kSortThreads; at < n; at += (uint64_t)gridDim.x * kSortThreads) {
+        const uint64_t i = at + threadIdx.x;
+        const bool live = i < n;
+        uint32_t key = 0;
+        if (live) {
+            const uint32_t b = __ldg(&bk.box_of[i]);
+            const DevParams *P = &bk.box[b];
+            const float4 p = __ldg(&pos[i]);
+            const float cell = __ldg(&P->cell);
+            const uint32_t dx = __ldg(&P->dims[0]), dy = __ldg(&P->dims[1]), dz = __ldg(&P->dims[2]);
+            const uint32_t cx = axis_cell(p.x, __ldg(&P->box_min[0]), cell, dx);
+            const uint32_t cy = axis_cell(p.y, __ldg(&P->box_min[1]), cell, dy);
+            const uint32_t cz = axis_cell(p.z, __ldg(&P->box_min[2]), cell, dz);
+            key = __ldg(&bk.cell_base[b]) + (cz * dy + cy) * dx + cx;
+            keys[i] = key;
+        }
+        count_digits(h, passes, live, key);
     }
-    const uint32_t act = __ballot_sync(0xffffffffu, live);
-    if (live) {
-        const uint32_t peers = __match_any_sync(act, key);
-        if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&counts[key], __popc(peers));
-    }
+    flush_digits(h, passes, digit_counts);
 }
 
-// Exclusive scan of in[0..n) into out[0..n), single pass. Tiles are claimed
-// in launch order through ctl[0]; ctl[1 + t] is tile t's status word: flag in
-// the high half (1 aggregate, 2 inclusive prefix), value in the low half.
-// With write_total, out[n] receives the grand total. With zero_in, the
-// input is cleared after it is read (the counts die here, as the
-// reference's scatter clears them for the next rebuild).
+// Combine of the single-pass scan: sum, or max (kMax); 0 is the identity of
+// both on unsigned values.
+template <bool kMax>
+__device__ __forceinline__ uint32_t scan_op(uint32_t a, uint32_t b) {
+    return kMax ? max(a, b) : a + b;
+}
+template <bool kMax>
+__device__ __forceinline__ uint32_t warp_reduce(uint32_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = scan_op<kMax>(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Scan of in[0..n) into out[0..n), single pass: exclusive sums, or with
+// kMax inclusive maxima. Tiles are claimed in launch order through ctl[0];
+// ctl[1 + t] is tile t's status word: flag in the high half (1 aggregate,
+// 2 inclusive prefix), value in the low half. With write_total, out[n]
+// receives the grand total. With zero_in, the input is cleared after it is
+// read.
+template <bool kMax>
 __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(uint32_t *in, uint32_t *out,
                                                                 uint32_t n,
                                                                 unsigned long long *ctl,
@@ -150,15 +215,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(uint32_t *in, ui
     }
     uint32_t sum = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) sum += v[k];
+    for (int k = 0; k < kScanItems; ++k) sum = scan_op<kMax>(sum, v[k]);
 
     // block-wide scan of the thread sums
     uint32_t x = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-        if (lane >= (uint32_t)o) x += y;
+        if (lane >= (uint32_t)o) x = scan_op<kMax>(x, y);
     }
+    uint32_t x_before = __shfl_up_sync(0xffffffffu, x, 1);
+    if (lane == 0) x_before = 0u;
     if (lane == 31) s_warp[warp] = x;
     __syncthreads();
     if (warp == 0) {
@@ -166,13 +233,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(uint32_t *in, ui
 #pragma unroll
         for (int o = 1; o < kScanThreads / 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= (uint32_t)o) w += y;
+            if (lane >= (uint32_t)o) w = scan_op<kMax>(w, y);
         }
         if (lane < kScanThreads / 32) s_warp[lane] = w;
     }
     __syncthreads();
     const uint32_t block_total = s_warp[kScanThreads / 32 - 1];
-    const uint32_t thread_excl = (warp > 0 ? s_warp[warp - 1] : 0u) + x - sum;
+    const uint32_t thread_excl = scan_op<kMax>(warp > 0 ? s_warp[warp - 1] : 0u, x_before);
 
     // decoupled look-back, warp 0
     if (warp == 0) {
@@ -200,24 +267,30 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(uint32_t *in, ui
                 const uint32_t val = (uint32_t)st;
                 if (pmask) {
                     const int j = __ffs(pmask) - 1;
-                    exclusive += warp_sum_u32((int)lane <= j ? val : 0u);
+                    exclusive = scan_op<kMax>(exclusive, warp_reduce<kMax>((int)lane <= j ? val : 0u));
                     break;
                 }
-                exclusive += warp_sum_u32(val);
+                exclusive = scan_op<kMax>(exclusive, warp_reduce<kMax>(val));
                 pred -= 32;
             }
-            if (lane == 0) st_relaxed(&status[tile], kFlagPrefix | (unsigned long long)(exclusive + block_total));
+            if (lane == 0)
+                st_relaxed(&status[tile], kFlagPrefix | (unsigned long long)scan_op<kMax>(exclusive, block_total));
         }
         if (lane == 0) s_excl = exclusive;
     }
     __syncthreads();
-    uint32_t run = s_excl + thread_excl;
+    uint32_t run = scan_op<kMax>(s_excl, thread_excl);
     if (vec) {
         uint32_t o[kScanItems];
 #pragma unroll
         for (int k = 0; k < kScanItems; ++k) {
-            o[k] = run;
-            run += v[k];
+            if (kMax) {
+                run = max(run, v[k]);
+                o[k] = run;
+            } else {
+                o[k] = run;
+                run += v[k];
+            }
         }
         uint4 *dst = reinterpret_cast<uint4 *>(out + base);
 #pragma unroll
@@ -231,74 +304,76 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(uint32_t *in, ui
     } else {
 #pragma unroll
         for (int k = 0; k < kScanItems; ++k) {
+            if (kMax) run = max(run, v[k]);
             if (base + k < n) {
                 out[base + k] = run;
                 if (zero_in) in[base + k] = 0u;
             }
-            run += v[k];
+            if (!kMax) run += v[k];
         }
     }
     if (write_total && threadIdx.x == 0 && (uint64_t)(tile + 1) * kScanTile >= n)
-        out[n] = s_excl + block_total;
+        out[n] = scan_op<kMax>(s_excl, block_total);
 }
 
-// Digit histogram of one tile of keys, written bin-major: hist[d * tiles + t].
-__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t *__restrict__ keys,
-                                                             uint32_t n, int shift,
-                                                             uint32_t *__restrict__ hist,
-                                                             uint32_t tiles) {
-    __shared__ uint32_t h[kRadix];
-    h[threadIdx.x] = 0;
-    __syncthreads();
-    const uint32_t tile = blockIdx.x;
-    const uint64_t base = (uint64_t)tile * kSortTile;
-#pragma unroll 4
-    for (int r = 0; r < kSortItems; ++r) {
-        const uint64_t i = base + (uint64_t)r * kSortThreads + threadIdx.x;
-        const bool live = i < n;
-        const uint32_t d = live ? (__ldg(&keys[i]) >> shift) & (kRadix - 1) : 0u;
-        const uint32_t act = __ballot_sync(0xffffffffu, live);
-        if (live) {
-            const uint32_t peers = __match_any_sync(act, d);
-            if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) atomicAdd(&h[d], __popc(peers));
-        }
-    }
-    __syncthreads();
-    hist[(uint64_t)threadIdx.x * tiles + tile] = h[threadIdx.x];
-}
-
-// Stable scatter of one digit pass. Warp w of tile t owns the contiguous
-// run t*TILE + w*32*ITEMS .. +32*ITEMS; in round r lane l holds element
-// run + r*32 + l, so (warp, round, lane) is input order and ranks taken in
-// that order keep equal digits in input order. `vals_in` null means the
-// identity (the first pass). `keys_out` may be null (the last pass).
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
-    const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t n,
-    int shift, const uint32_t *__restrict__ offsets, uint32_t tiles,
-    uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out) {
+// One stable digit pass. Tiles are claimed in launch order through
+// *tile_ctr. Warp w of tile t owns the contiguous run t*TILE + w*32*ITEMS ..
+// +32*ITEMS; in round r lane l holds element run + r*32 + l, so (warp,
+// round, lane) is input order and ranks taken in that order keep equal
+// digits in input order. The tile's count of each digit d is published in
+// tile_status[t][d] (flag in the high half: 1 this tile's count, 2 the
+// inclusive count over tiles 0..t), and the thread of digit d looks back
+// over the tiles before it for their counts of d (decoupled look-back, one
+// chain per digit, every spin bounded). A digit's output run starts at the
+// number of smaller digits over all keys (digit_counts) plus its count in
+// earlier tiles. The tile is laid out in shared memory in (digit, input)
+// order and written out by consecutive threads to consecutive addresses.
+// `vals_in` null means the identity (the first pass); `keys_out` may be
+// null (the last pass). With `starts` (the last pass, keys now in final
+// order) every run of equal keys also stores its end at starts[key + 1]:
+// inside a tile's digit segment the next output element is the next staged
+// one, and the last element of a segment, whose successor another tile
+// writes, stores with atomicMax (the true end of its run is larger).
+static_assert(kRadix == kSortThreads, "one thread per digit");
+#ifndef FCU_SORT_MINB
+#define FCU_SORT_MINB 4
+#endif
+__global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
+    const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t n, int shift,
+    const uint32_t *__restrict__ digit_counts, unsigned long long *tile_status, uint32_t *tile_ctr,
+    uint32_t *err, uint32_t *__restrict__ keys_out, uint32_t *__restrict__ vals_out,
+    uint32_t *__restrict__ starts, uint32_t cells) {
     __shared__ uint32_t s_hist[kSortWarps][kRadix];
-    __shared__ uint32_t s_off[kRadix];
+    __shared__ uint32_t s_off[kRadix];    // output index of this tile's first element of digit d
+    __shared__ uint32_t s_start[kRadix];  // staged index of the tile's first element of digit d
+    __shared__ uint32_t s_wsum[kSortWarps];
+    __shared__ uint32_t s_gsum[kSortWarps];
+    __shared__ uint32_t s_key[kSortTile];
+    __shared__ uint32_t s_val[kSortTile];
+    __shared__ uint32_t s_tile;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t tile = blockIdx.x;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
 #pragma unroll
     for (int w = 0; w < kSortWarps; ++w) s_hist[w][threadIdx.x] = 0;
-    s_off[threadIdx.x] = offsets[(uint64_t)threadIdx.x * tiles + tile];
     __syncthreads();
+    const uint32_t tile = s_tile;
 
     const uint64_t wbase = (uint64_t)tile * kSortTile + (uint64_t)warp * (32 * kSortItems);
     const uint32_t lt = lanemask_lt();
-    uint32_t key[kSortItems], val[kSortItems], rank[kSortItems];
+    uint32_t key[kSortItems], rank[kSortItems];
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const uint64_t i = wbase + (uint64_t)r * 32 + lane;
-        const bool live = i < n;
-        key[r] = live ? __ldg(&keys_in[i]) : 0u;
-        val[r] = live ? (vals_in ? __ldg(&vals_in[i]) : (uint32_t)i) : 0u;
+        key[r] = i < n ? __ldg(&keys_in[i]) : 0u;
+    }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const bool live = wbase + (uint64_t)r * 32 + lane < n;
         const uint32_t d = (key[r] >> shift) & (kRadix - 1);
         const uint32_t act = __ballot_sync(0xffffffffu, live);
+        const uint32_t peers = digit_peers(act, d);
         rank[r] = 0;
         if (live) {
-            const uint32_t peers = __match_any_sync(act, d);
             const uint32_t before = s_hist[warp][d];
             rank[r] = before + __popc(peers & lt);
             __syncwarp(act);
@@ -307,27 +382,92 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
         __syncwarp();
     }
     __syncthreads();
-    {
-        uint32_t run = 0;
+    // thread = digit d: the warps' exclusive counts of it, and its tile count
+    const uint32_t dig = threadIdx.x;
+    uint32_t total = 0;
 #pragma unroll
-        for (int w = 0; w < kSortWarps; ++w) {
-            const uint32_t t = s_hist[w][threadIdx.x];
-            s_hist[w][threadIdx.x] = run;
-            run += t;
+    for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t t = s_hist[w][dig];
+        s_hist[w][dig] = total;
+        total += t;
+    }
+    unsigned long long *mine = tile_status + (uint64_t)tile * kRadix;
+    st_relaxed(&mine[dig], (tile == 0 ? kFlagPrefix : kFlagAgg) | total);
+
+    // exclusive scans over the digits: of the tile counts (staged starts)
+    // and of the global counts (where each digit's output begins)
+    const uint32_t gc = __ldg(&digit_counts[dig]);
+    uint32_t x = total, y = gc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t xu = __shfl_up_sync(0xffffffffu, x, o);
+        const uint32_t yu = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= (uint32_t)o) {
+            x += xu;
+            y += yu;
         }
     }
+    if (lane == 31) {
+        s_wsum[warp] = x;
+        s_gsum[warp] = y;
+    }
+
+    // look-back over the earlier tiles' counts of this digit
+    uint32_t excl = 0;
+    if (tile > 0) {
+        int64_t pred = (int64_t)tile - 1;
+        while (pred >= 0) {
+            unsigned long long v = ld_relaxed(&tile_status[(uint64_t)pred * kRadix + dig]);
+            uint32_t spins = 0;
+            while ((v >> 32) == 0) {
+                if (++spins > kSpinLimit) {
+                    atomicOr(err, ERRF_SCAN_TIMEOUT);
+                    v = kFlagPrefix;  // give up: count it as zero and stop
+                    break;
+                }
+                v = ld_relaxed(&tile_status[(uint64_t)pred * kRadix + dig]);
+            }
+            excl += (uint32_t)v;
+            if ((v >> 32) == 2ull) break;
+            --pred;
+        }
+        st_relaxed(&mine[dig], kFlagPrefix | (unsigned long long)(excl + total));
+    }
+    __syncthreads();
+    uint32_t wx = 0, wy = 0;
+    for (uint32_t w = 0; w < warp; ++w) {
+        wx += s_wsum[w];
+        wy += s_gsum[w];
+    }
+    s_start[dig] = wx + x - total;
+    s_off[dig] = wy + y - gc + excl;
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const uint64_t i = wbase + (uint64_t)r * 32 + lane;
         if (i < n) {
             const uint32_t d = (key[r] >> shift) & (kRadix - 1);
-            const uint32_t dst = s_off[d] + s_hist[warp][d] + rank[r];
-            // Always below n when the offsets are right; the test keeps a
-            // scan that gave up (garbage offsets) from writing out of bounds.
-            if (dst < n) {
-                vals_out[dst] = val[r];
-                if (keys_out) keys_out[dst] = key[r];
+            const uint32_t at = s_start[d] + s_hist[warp][d] + rank[r];
+            s_key[at] = key[r];
+            s_val[at] = vals_in ? __ldg(&vals_in[i]) : (uint32_t)i;
+        }
+    }
+    __syncthreads();
+    const uint64_t tbase = (uint64_t)tile * kSortTile;
+    const uint32_t count = (uint32_t)(n - tbase < kSortTile ? n - tbase : kSortTile);
+    for (uint32_t j = threadIdx.x; j < count; j += kSortThreads) {
+        const uint32_t k = s_key[j];
+        const uint32_t d = (k >> shift) & (kRadix - 1);
+        const uint32_t dst = s_off[d] + (j - s_start[d]);
+        // Always below n when the counts are right; the test keeps a
+        // look-back that gave up (garbage offsets) from writing out of bounds.
+        if (dst < n) {
+            vals_out[dst] = s_val[j];
+            if (keys_out) keys_out[dst] = k;
+            if (starts && k < cells) {
+                const bool seg_end = j + 1 == count || ((s_key[j + 1] >> shift) & (kRadix - 1)) != d;
+                if (seg_end) atomicMax(&starts[k + 1], dst + 1);
+                else if (s_key[j + 1] != k) starts[k + 1] = dst + 1;
             }
         }
     }
@@ -339,15 +479,40 @@ size_t scan_region_bytes(uint32_t len) {
     return align256(8ull * (1ull + div_up(len, kScanTile)));
 }
 
+// The zeroed part of the workspace: the starts scan's look-back region,
+// every pass's tile counter and tile status words, every pass's digit
+// counts.
+struct SortRegion {
+    unsigned long long *fill_ctl;
+    uint32_t *tile_ctr[kMaxPasses];
+    unsigned long long *tile_status[kMaxPasses];
+    uint32_t *digit_counts;
+    size_t bytes;
+};
+
+SortRegion sort_region(void *base, uint32_t n, uint32_t cells, int passes) {
+    SortRegion r{};
+    const uint32_t tiles = div_up(n > 0 ? n : 1, kSortTile);
+    const uintptr_t b = reinterpret_cast<uintptr_t>(base);
+    size_t off = 0;
+    r.fill_ctl = reinterpret_cast<unsigned long long *>(b + off);
+    off += scan_region_bytes(cells + 1);
+    for (int q = 0; q < passes; ++q) {
+        r.tile_ctr[q] = reinterpret_cast<uint32_t *>(b + off);
+        off += 256;
+        r.tile_status[q] = reinterpret_cast<unsigned long long *>(b + off);
+        off += align256(8ull * kRadix * tiles);
+    }
+    r.digit_counts = reinterpret_cast<uint32_t *>(b + off);
+    off += align256(4ull * kRadix * kMaxPasses);
+    r.bytes = off;
+    return r;
+}
+
 }  // namespace
 
 size_t grid_work_bytes(uint32_t n, uint32_t cells) {
-    const int passes = radix_passes(cells);
-    const uint32_t tiles = div_up(n > 0 ? n : 1, kSortTile);
-    size_t b = 0;
-    b += align256(4ull * cells);
-    b += scan_region_bytes(cells) + (size_t)passes * scan_region_bytes(kRadix * tiles);
-    b += align256(4ull * kRadix * tiles);
+    size_t b = sort_region(nullptr, n, cells, radix_passes(cells)).bytes;
     b += 4 * align256(4ull * (n > 0 ? n : 1));
     b += 256;  // err word when the caller gives none
     return b;
@@ -358,15 +523,10 @@ GridWork grid_work_carve(void *ws, uint32_t n, uint32_t cells, uint32_t *err) {
     w.passes = radix_passes(cells);
     w.cells = cells;
     w.n = n;
-    const uint32_t tiles = div_up(n > 0 ? n : 1, kSortTile);
     char *p = (char *)ws;
-    w.counts = (uint32_t *)p;
-    p += align256(4ull * cells);
     w.scan_ctl = (unsigned long long *)p;
-    w.scan_ctl_bytes = scan_region_bytes(cells) + (size_t)w.passes * scan_region_bytes(kRadix * tiles);
+    w.scan_ctl_bytes = sort_region(ws, n, cells, w.passes).bytes;
     p += w.scan_ctl_bytes;
-    w.hist = (uint32_t *)p;
-    p += align256(4ull * kRadix * tiles);
     const size_t nb = align256(4ull * (n > 0 ? n : 1));
     w.k1 = (uint32_t *)p;
     p += nb;
@@ -382,46 +542,41 @@ GridWork grid_work_carve(void *ws, uint32_t n, uint32_t cells, uint32_t *err) {
 
 cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t n,
                                const GridGeom &g, uint32_t *keys, uint32_t *starts,
-                               uint32_t *perm, GridWork &w, bool counts_zeroed,
-                               const DevStep *ring, DevStep *cur, DevSolve *solve,
-                               uint32_t ring_size, const BoxKeys *boxes) {
+                               uint32_t *perm, GridWork &w, const DevStep *ring, DevStep *cur,
+                               DevSolve *solve, uint32_t ring_size, const BoxKeys *boxes) {
     cudaError_t e;
     const uint32_t cells = w.cells;
-    if (!counts_zeroed) {
-        e = cudaMemsetAsync(w.counts, 0, 4ull * cells, stream);
-        if (e != cudaSuccess) return e;
-    }
+    const SortRegion r = sort_region(w.scan_ctl, n, cells, w.passes);
     e = cudaMemsetAsync(w.scan_ctl, 0, w.scan_ctl_bytes, stream);
     if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(starts, 0, 4ull * cells + 4, stream);
+    if (e != cudaSuccess) return e;
     if (n > 0 || ring) {
-        const uint32_t blocks = div_up(n > 0 ? n : 1, 256);
+        const uint32_t blocks = std::min(div_up(n > 0 ? n : 1, kSortThreads), kKeyBlocks);
         if (boxes)
-            k_box_keys<<<blocks, 256, 0, stream>>>(pos, n, *boxes, keys, w.counts, ring, cur, solve, ring_size);
+            k_box_keys<<<blocks, kSortThreads, 0, stream>>>(pos, n, *boxes, keys, w.passes, r.digit_counts, ring,
+                                                            cur, solve, ring_size);
         else
-            k_cell_keys<<<blocks, 256, 0, stream>>>(pos, n, g, keys, w.counts, ring, cur, solve, ring_size);
+            k_cell_keys<<<blocks, kSortThreads, 0, stream>>>(pos, n, g, keys, w.passes, r.digit_counts, ring, cur,
+                                                             solve, ring_size);
     }
-    unsigned long long *ctl = w.scan_ctl;
-    k_scan_lookback<<<div_up(cells > 0 ? cells : 1, kScanTile), kScanThreads, 0, stream>>>(
-        w.counts, starts, cells, ctl, w.err, 1, 1);
-    ctl += scan_region_bytes(cells) / 8;
-    if (n == 0) return cudaGetLastError();
-    const uint32_t tiles = div_up(n, kSortTile);
-    const uint32_t *kin = keys;
-    const uint32_t *vin = nullptr;
-    for (int pass = 0; pass < w.passes; ++pass) {
-        const int shift = pass * kRadixBits;
-        const bool last = pass == w.passes - 1;
-        uint32_t *kout = last ? nullptr : ((pass & 1) ? w.k2 : w.k1);
-        uint32_t *vout = last ? perm : ((pass & 1) ? w.v2 : w.v1);
-        k_radix_hist<<<tiles, kSortThreads, 0, stream>>>(kin, n, shift, w.hist, tiles);
-        const uint32_t len = kRadix * tiles;
-        k_scan_lookback<<<div_up(len, kScanTile), kScanThreads, 0, stream>>>(w.hist, w.hist, len, ctl,
-                                                                             w.err, 0, 0);
-        ctl += scan_region_bytes(len) / 8;
-        k_radix_scatter<<<tiles, kSortThreads, 0, stream>>>(kin, vin, n, shift, w.hist, tiles, kout, vout);
-        kin = kout;
-        vin = vout;
+    if (n > 0) {
+        const uint32_t tiles = div_up(n, kSortTile);
+        const uint32_t *kin = keys;
+        const uint32_t *vin = nullptr;
+        for (int pass = 0; pass < w.passes; ++pass) {
+            const bool last = pass == w.passes - 1;
+            uint32_t *kout = last ? nullptr : ((pass & 1) ? w.k2 : w.k1);
+            uint32_t *vout = last ? perm : ((pass & 1) ? w.v2 : w.v1);
+            k_radix_pass<<<tiles, kSortThreads, 0, stream>>>(
+                kin, vin, n, pass * kRadixBits, r.digit_counts + pass * kRadix, r.tile_status[pass],
+                r.tile_ctr[pass], w.err, kout, vout, last ? starts : nullptr, cells);
+            kin = kout;
+            vin = vout;
+        }
     }
+    k_scan_lookback<true><<<div_up(cells + 1ull, kScanTile), kScanThreads, 0, stream>>>(starts, starts, cells + 1,
+                                                                                        r.fill_ctl, w.err, 0, 0);
     return cudaGetLastError();
 }
 
@@ -460,7 +615,7 @@ extern "C" int32_t fluid_selftest_scan_wait(int32_t device, float *ms) {
         if ((e = cudaEventCreate(&ev[0])) != cudaSuccess) break;
         if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) break;
         cudaEventRecord(ev[0]);
-        k_scan_lookback<<<1, kScanThreads>>>(in, out, n, ctl, err, 0, 0);
+        k_scan_lookback<false><<<1, kScanThreads>>>(in, out, n, ctl, err, 0, 0);
         cudaEventRecord(ev[1]);
         if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) break;
         if ((e = cudaGetLastError()) != cudaSuccess) break;

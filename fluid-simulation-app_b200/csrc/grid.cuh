@@ -21,6 +21,8 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortItems = 16;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kMaxPasses = 4;                               // 32-bit keys
+constexpr uint32_t kKeyBlocks = 148 * 8;                    // grid cap of the key kernels
 
 inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
@@ -38,10 +40,8 @@ inline int radix_passes(uint32_t cells) {
 
 // Scratch of one grid build, carved from one device allocation.
 struct GridWork {
-    uint32_t *counts;              // [cells], zero between builds
-    unsigned long long *scan_ctl;  // (1 + passes) look-back regions, zeroed per build
+    unsigned long long *scan_ctl;  // look-back words and digit counts, zeroed per build
     size_t scan_ctl_bytes;
-    uint32_t *hist;                // [kRadix * tiles]
     uint32_t *k1, *k2, *v1, *v2;   // ping-pong keys / values
     uint32_t *err;                 // device error word (may alias the sim's)
     int passes;
@@ -62,17 +62,16 @@ struct BoxKeys {
     uint32_t nboxes;
 };
 
-// Enqueues count -> scan -> stable sort on `stream`. `keys` receives each
-// input's cell key, `starts` the exclusive scan with starts[cells] = n,
-// `perm` the stable permutation. When `counts_zeroed` is false the counts
-// are cleared first. `ring`/`cur`/`solve` (may be null) let the key kernel
+// Enqueues keys -> stable radix sort -> starts on `stream`. `keys` receives
+// each input's cell key, `starts` the exclusive scan of the cell counts with
+// starts[cells] = n, `perm` the stable permutation. `ring`/`cur`/`solve`
+// (may be null) let the key kernel
 // also fetch the substep's Step block from the ring. With `boxes`, the keys
 // are the batch's (`g` unused) and every box's Step block of the substep
 // (ring entry cursor holds nboxes of them) moves to cur[0 .. nboxes-1].
 cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t n,
                                const GridGeom &g, uint32_t *keys, uint32_t *starts,
-                               uint32_t *perm, GridWork &w, bool counts_zeroed,
-                               const DevStep *ring, DevStep *cur, DevSolve *solve,
-                               uint32_t ring_size, const BoxKeys *boxes = nullptr);
+                               uint32_t *perm, GridWork &w, const DevStep *ring, DevStep *cur,
+                               DevSolve *solve, uint32_t ring_size, const BoxKeys *boxes = nullptr);
 
 }  // namespace fcu

@@ -114,8 +114,8 @@ extern "C" int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const 
     }
     g.cell = grid->cell;
     if (e == cudaSuccess)
-        e = grid_build_enqueue(st, (const float4 *)pos4, n, g, keys ? keys : w.k2, starts, perm, w, false,
-                               nullptr, nullptr, nullptr, 1);
+        e = grid_build_enqueue(st, (const float4 *)pos4, n, g, keys ? keys : w.k2, starts, perm, w, nullptr,
+                               nullptr, nullptr, 1);
     if (e != cudaSuccess)
         return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static: ") + cudaGetErrorString(e));
     return FLUID_OK;

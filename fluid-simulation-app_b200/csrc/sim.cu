@@ -303,7 +303,7 @@ cudaError_t enqueue_substep(FluidSim *s, cudaStream_t st, uint32_t div_iters, ui
     cudaError_t e = cudaMemsetAsync(s->solve->acc_div, 0, 2 * kAccSlots * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     e = grid_build_enqueue(st, s->b.pos, s->n, geom_of(s->P), s->b.keys, s->b.starts, s->b.perm, s->gw,
-                           true, s->ring, s->cur, s->solve, kRing);
+                           s->ring, s->cur, s->solve, kRing);
     if (e != cudaSuccess) return e;
     mark("grid");
     const Geo g = s->geo();
@@ -399,7 +399,7 @@ int32_t capture_tolerance(FluidSim *s, cudaGraphExec_t *out) {
     cudaError_t e = cudaMemsetAsync(s->solve->acc_div, 0, 2 * kAccSlots * sizeof(unsigned long long), st);
     if (e == cudaSuccess)
         e = grid_build_enqueue(st, s->b.pos, s->n, geom_of(s->P), s->b.keys, s->b.starts, s->b.perm, s->gw,
-                               true, s->ring, s->cur, s->solve, kRing);
+                               s->ring, s->cur, s->solve, kRing);
     const Geo geo = s->geo();
     // With at least one divergence apply, forces_eval runs after every one
     // and also forms the divergence prediction that decides whether the
@@ -707,7 +707,6 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(cudaMemset(b.stats_acc, 0, 8));
     CK(cudaMemset(b.stats, 0, 64));
     CK(cudaMemset(s->solve, 0, sizeof(DevSolve)));
-    CK(cudaMemset(s->gw.counts, 0, 4 * C));
     if (s->ntr) {
         std::vector<uint32_t> tr;
         seed_tracers(*cfg, s->P, s->ntr, tr);
@@ -1038,11 +1037,11 @@ int32_t fluid_sim_read_field(FluidSim *s, int32_t field, void *out, uint64_t byt
 uint32_t fluid_sim_kernels_per_substep(const FluidSim *s) {
     if (!s) return 0;
     const uint32_t passes = (uint32_t)radix_passes(s->cells);
-    // keys + scan + 3 per radix pass + gather + density_div
+    // keys + one per radix pass + starts scan + gather + density_div
     //   + div applies (+ div_kappa after the first) + forces pair
     //   + den pairs + integrate
     const uint32_t d = s->cfg.div_iters, k = s->cfg.den_iters;
-    return 2 + 3 * passes + 1 + 1 + (d ? 2 * d - 1 : 0) + 2 + 2 * k + 1;
+    return 2 + passes + 1 + 1 + (d ? 2 * d - 1 : 0) + 2 + 2 * k + 1;
 }
 
 int32_t fluid_sim_profile_step(FluidSim *s, const FluidStep *step, float *ms, const char **names,
@@ -1162,8 +1161,8 @@ int32_t fluid_grid_build(const float *pos4, uint32_t n, const FluidGrid *grid, u
         g.dims[i] = grid->dims[i];
     }
     g.cell = grid->cell;
-    CK(grid_build_enqueue(st, (const float4 *)pos4, n, g, k, starts, perm, w, false, nullptr, nullptr,
-                          nullptr, kRing));
+    CK(grid_build_enqueue(st, (const float4 *)pos4, n, g, k, starts, perm, w, nullptr, nullptr, nullptr,
+                          kRing));
     return FLUID_OK;
 }
 

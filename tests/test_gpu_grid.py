@@ -13,25 +13,6 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def positions(kind, n, side, seed):
-    rng = np.random.default_rng(seed)
-    p = np.zeros((n, 4), np.float32)
-    if kind == "uniform":
-        p[:, :3] = rng.uniform(0, side, (n, 3))
-    elif kind == "packed":
-        k = int(n * 0.9)
-        p[:k, :3] = rng.uniform(0, side, (k, 3))
-        p[:k, 1] = rng.uniform(0, side * 0.1, k)
-        p[k:, :3] = rng.uniform(0, side, (n - k, 3))
-    elif kind == "gaussian":
-        centres = rng.uniform(side / 8, side * 7 / 8, (8, 3))
-        per = n // 8
-        for c in range(8):
-            m = per if c < 7 else n - 7 * per
-            p[c * per:c * per + m, :3] = centres[c] + rng.normal(0, 4.0, (m, 3))
-    return p
-
-
 def grid(orc, fcu, side):
     g = fcu.FluidGrid()
     g.min[:] = [0.0, 0.0, 0.0]
@@ -45,10 +26,10 @@ def grid(orc, fcu, side):
 
 
 @pytest.mark.parametrize("kind", ["uniform", "packed", "gaussian"])
-def test_grid_is_the_stable_counting_sort(orc, fcu, kind):
+def test_grid_is_the_stable_counting_sort(orc, fcu, wl, kind):
     side = 64
     g, og = grid(orc, fcu, side)
-    pos = positions(kind, 1 << 20, side, seed={"uniform": 1, "packed": 2, "gaussian": 3}[kind])
+    pos = wl.grid_positions(kind, 1 << 20, side, seed={"uniform": 1, "packed": 2, "gaussian": 3}[kind])
     starts, perm = fcu.grid_build_host(pos, g)
     keys, e_starts, e_perm = orc.grid_build(og, pos)
     assert starts[-1] == len(pos)
@@ -57,17 +38,17 @@ def test_grid_is_the_stable_counting_sort(orc, fcu, kind):
 
 
 @pytest.mark.parametrize("kind", ["uniform", "packed", "gaussian"])
-def test_grid_at_full_size_16m_positions_in_2_24_cells(orc, fcu, kind):
+def test_grid_at_full_size_16m_positions_in_2_24_cells(orc, fcu, wl, kind):
     side = 256
     g, og = grid(orc, fcu, side)
-    pos = positions(kind, 1 << 24, side, seed={"uniform": 1, "packed": 2, "gaussian": 3}[kind])
+    pos = wl.grid_positions(kind, 1 << 24, side, seed={"uniform": 1, "packed": 2, "gaussian": 3}[kind])
     starts, perm = fcu.grid_build_host(pos, g)
     keys, e_starts, e_perm = orc.grid_build(og, pos)
     assert np.array_equal(starts, e_starts)
     assert np.array_equal(perm, e_perm)
 
 
-def test_grid_edge_cases(orc, fcu):
+def test_grid_edge_cases(orc, fcu, wl):
     side = 16
     g, og = grid(orc, fcu, side)
     cases = {
@@ -75,8 +56,8 @@ def test_grid_edge_cases(orc, fcu):
         "all_in_one_cell": np.tile(np.array([[5.5, 5.5, 5.5, 0]], np.float32), (20000, 1)),
         "outside_and_nan": np.array([[-5, 1, 1, 0], [100, 100, 100, 0], [np.nan, 1, 1, 0],
                                      [1, -np.inf, np.inf, 0], [15.999, 0, 0, 0]] * 1000, np.float32),
-        "ragged": positions("uniform", 4097, side, 9),
-        "tile_edge": positions("gaussian", 4096 * 3, side, 10),
+        "ragged": wl.grid_positions("uniform", 4097, side, 9),
+        "tile_edge": wl.grid_positions("gaussian", 4096 * 3, side, 10),
     }
     for name, pos in cases.items():
         starts, perm = fcu.grid_build_host(pos, g)
@@ -94,11 +75,11 @@ def test_grid_with_no_positions(fcu):
     assert np.all(starts == 0) and len(perm) == 0
 
 
-def test_grid_on_device_pointers_in_a_caller_stream(orc, fcu):
+def test_grid_on_device_pointers_in_a_caller_stream(orc, fcu, wl):
     import torch
     side = 128
     g, og = grid(orc, fcu, side)
-    pos = positions("gaussian", 1 << 21, side, 5)
+    pos = wl.grid_positions("gaussian", 1 << 21, side, 5)
     d_pos = torch.from_numpy(pos).cuda()
     n = pos.shape[0]
     C = side ** 3
