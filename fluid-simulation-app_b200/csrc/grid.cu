@@ -335,8 +335,16 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_lookback(uint32_t *in, ui
 // one, and the last element of a segment, whose successor another tile
 // writes, stores with atomicMax (the true end of its run is larger).
 static_assert(kRadix == kSortThreads, "one thread per digit");
+// Blocks per SM the pass kernel is compiled for: 4 (64 registers) measured
+// 0.75 ms at 16.7M positions against 0.84 at 3 and 1.01 at 1.
 #ifndef FCU_SORT_MINB
 #define FCU_SORT_MINB 4
+#endif
+// FCU_SORT_MATCH: digit peers by __match_any_sync instead of eight ballots.
+// Measured at 16.7M positions: 15 % slower on uniform keys, 4 % faster on
+// clustered ones; the simulation's grid 6 % faster.
+#ifndef FCU_SORT_MATCH
+#define FCU_SORT_MATCH 0
 #endif
 __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
     const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t n, int shift,
@@ -371,7 +379,11 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
         const bool live = wbase + (uint64_t)r * 32 + lane < n;
         const uint32_t d = (key[r] >> shift) & (kRadix - 1);
         const uint32_t act = __ballot_sync(0xffffffffu, live);
+#if FCU_SORT_MATCH
+        const uint32_t peers = live ? __match_any_sync(act, d) : 0u;
+#else
         const uint32_t peers = digit_peers(act, d);
+#endif
         rank[r] = 0;
         if (live) {
             const uint32_t before = s_hist[warp][d];
