@@ -15,7 +15,8 @@ events; the state lives in HBM (working set ~0.5 GB, past the 126 MB L2, so
 no flush is needed). e2e: the same frames through the C ABI with a stats
 read back to host memory after every frame, wall-clocked. roofline: the
 dominant kernel, timed kernel by kernel with CUDA events on the sim's
-stream. cpu_baseline: the CPU oracle on this host's cores over a bounded
+stream, against the peak (MEASURED_PEAKS.json, else the 6.65 TB/s fallback)
+and against a device-to-device copy measured in the same run. cpu_baseline: the CPU oracle on this host's cores over a bounded
 sample (one substep of the same state). N > 1: one independent replica per
 GPU (a single box does not shard), max over ranks.
 
