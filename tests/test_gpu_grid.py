@@ -102,3 +102,32 @@ def test_grid_on_device_pointers_in_a_caller_stream(orc, fcu, wl):
                           stream.cuda_stream)
     stream.synchronize()
     assert np.array_equal(perm.cpu().numpy().view(np.uint32), e_perm)
+
+
+@pytest.mark.parametrize("dims,passes", [((4, 4, 4), 1), ((40, 40, 40), 2), ((256, 256, 256), 3),
+                                         ((512, 256, 256), 4)])
+def test_grid_every_digit_pass_count(orc, fcu, wl, dims, passes):
+    """1 to 4 eight-bit digit passes (keys below 2^8, 2^16, 2^24, 2^25): the
+    last pass writes the run ends, so each count is checked, with keys
+    clustered enough that runs of equal keys cross tile boundaries."""
+    cells = dims[0] * dims[1] * dims[2]
+    assert passes == max(1, ((cells - 1).bit_length() + 7) // 8)
+    g = fcu.FluidGrid()
+    g.min[:] = [0.0, 0.0, 0.0]
+    g.cell = 1.0
+    g.dims[:] = list(dims)
+    og = orc.OrGrid()
+    og.min[:] = [0.0, 0.0, 0.0]
+    og.cell = 1.0
+    og.dims[:] = list(dims)
+    rng = np.random.default_rng(passes)
+    n = 300_000
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(0, 1, (n, 3)) * np.array(dims, np.float32)
+    # a third of the points in a few cells: runs longer than a 4,096-key tile
+    k = n // 3
+    pos[:k, :3] = (rng.integers(0, 3, (k, 3)) + 0.5).astype(np.float32)
+    starts, perm = fcu.grid_build_host(pos, g)
+    _, e_starts, e_perm = orc.grid_build(og, pos)
+    assert np.array_equal(starts, e_starts)
+    assert np.array_equal(perm, e_perm)
