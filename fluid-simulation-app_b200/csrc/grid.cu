@@ -105,19 +105,29 @@ __global__ void __launch_bounds__(kSortThreads) k_cell_keys(const float4 *__rest
     }
     for (int p = 0; p < kMaxPasses; ++p) h[p][threadIdx.x] = 0;
     __syncthreads();
-    for (uint64_t at = (uint64_t)blockIdx.x * kSortThreads; at < n; at += (uint64_t)gridDim.x * kSortThreads) {
-        const uint64_t i = at + threadIdx.x;
-        const bool live = i < n;
-        uint32_t key = 0;
-        if (live) {
-            const float4 p = __ldg(&pos[i]);
-            const uint32_t cx = axis_cell(p.x, g.min[0], g.cell, g.dims[0]);
-            const uint32_t cy = axis_cell(p.y, g.min[1], g.cell, g.dims[1]);
-            const uint32_t cz = axis_cell(p.z, g.min[2], g.cell, g.dims[2]);
-            key = (cz * g.dims[1] + cy) * g.dims[0] + cx;
-            keys[i] = key;
+    // kKeyItems positions per thread and round, all loaded before any is used
+    const uint64_t stride = (uint64_t)gridDim.x * kSortThreads * kKeyItems;
+    for (uint64_t at = (uint64_t)blockIdx.x * kSortThreads * kKeyItems; at < n; at += stride) {
+        float4 p[kKeyItems];
+#pragma unroll
+        for (int u = 0; u < kKeyItems; ++u) {
+            const uint64_t i = at + (uint64_t)u * kSortThreads + threadIdx.x;
+            p[u] = i < n ? __ldg(&pos[i]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        count_digits(h, passes, live, key);
+#pragma unroll
+        for (int u = 0; u < kKeyItems; ++u) {
+            const uint64_t i = at + (uint64_t)u * kSortThreads + threadIdx.x;
+            const bool live = i < n;
+            uint32_t key = 0;
+            if (live) {
+                const uint32_t cx = axis_cell(p[u].x, g.min[0], g.cell, g.dims[0]);
+                const uint32_t cy = axis_cell(p[u].y, g.min[1], g.cell, g.dims[1]);
+                const uint32_t cz = axis_cell(p[u].z, g.min[2], g.cell, g.dims[2]);
+                key = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+                keys[i] = key;
+            }
+            count_digits(h, passes, live, key);
+        }
     }
     flush_digits(h, passes, digit_counts);
 }
@@ -564,7 +574,8 @@ cudaError_t grid_build_enqueue(cudaStream_t stream, const float4 *pos, uint32_t 
     e = cudaMemsetAsync(starts, 0, 4ull * cells + 4, stream);
     if (e != cudaSuccess) return e;
     if (n > 0 || ring) {
-        const uint32_t blocks = std::min(div_up(n > 0 ? n : 1, kSortThreads), kKeyBlocks);
+        const uint32_t per = boxes ? kSortThreads : kSortThreads * kKeyItems;
+        const uint32_t blocks = std::min(div_up(n > 0 ? n : 1, per), kKeyBlocks);
         if (boxes)
             k_box_keys<<<blocks, kSortThreads, 0, stream>>>(pos, n, *boxes, keys, w.passes, r.digit_counts, ring,
                                                             cur, solve, ring_size);

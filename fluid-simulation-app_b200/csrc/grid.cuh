@@ -23,6 +23,10 @@ constexpr int kSortItems = 16;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
 constexpr int kMaxPasses = 4;                               // 32-bit keys
 constexpr uint32_t kKeyBlocks = 148 * 8;                    // grid cap of the key kernels
+#ifndef FCU_KEY_ITEMS
+#define FCU_KEY_ITEMS 4
+#endif
+constexpr int kKeyItems = FCU_KEY_ITEMS;                    // positions per thread and round (cell keys)
 
 inline uint32_t div_up(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
