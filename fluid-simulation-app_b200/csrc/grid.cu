@@ -612,6 +612,65 @@ int32_t report_error(int32_t code, const std::string &msg);
 // which tile 0 never publishes, so its look-back polls status[0] until the
 // kSpinLimit bound, records ERRF_SCAN_TIMEOUT and treats the missing prefix
 // as zero. Nothing faults or hangs; the context stays usable.
+// One block of a radix digit pass that claims tile 1 while tile 0 never
+// publishes its digit counts: every digit's bounded look-back gives up. The
+// keys are all zero, so the give-up offsets still land inside the outputs.
+extern "C" int32_t fluid_selftest_radix_wait(int32_t device, float *ms) {
+    using namespace fcu;
+    auto fail = [](cudaError_t e) {
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_selftest_radix_wait: ") + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(e);
+    const uint32_t n = 2 * kSortTile;
+    uint32_t *keys = nullptr, *keys_out = nullptr, *vals_out = nullptr, *counts = nullptr, *ctr = nullptr,
+             *err = nullptr;
+    unsigned long long *status = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    uint32_t flags = 0;
+    float t = 0.0f;
+    const uint32_t one = 1u;
+    do {
+        if ((e = cudaMalloc(&keys, 4ull * n)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&keys_out, 4ull * n)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&vals_out, 4ull * n)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&counts, 4ull * kRadix)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&status, 8ull * kRadix * 2)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&ctr, 4)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&err, 4)) != cudaSuccess) break;
+        if ((e = cudaMemset(keys, 0, 4ull * n)) != cudaSuccess) break;
+        if ((e = cudaMemset(counts, 0, 4ull * kRadix)) != cudaSuccess) break;
+        if ((e = cudaMemset(status, 0, 8ull * kRadix * 2)) != cudaSuccess) break;
+        if ((e = cudaMemset(err, 0, 4)) != cudaSuccess) break;
+        if ((e = cudaMemcpy(ctr, &one, 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = cudaEventCreate(&ev[0])) != cudaSuccess) break;
+        if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) break;
+        cudaEventRecord(ev[0]);
+        k_radix_pass<<<1, kSortThreads>>>(keys, nullptr, n, 0, counts, status, ctr, err, keys_out, vals_out,
+                                          nullptr, 1u);
+        cudaEventRecord(ev[1]);
+        if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) break;
+        if ((e = cudaGetLastError()) != cudaSuccess) break;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        if ((e = cudaMemcpy(&flags, err, 4, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+    } while (false);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaFree(keys);
+    cudaFree(keys_out);
+    cudaFree(vals_out);
+    cudaFree(counts);
+    cudaFree(status);
+    cudaFree(ctr);
+    cudaFree(err);
+    if (e != cudaSuccess) return fail(e);
+    if (ms) *ms = t;
+    if (flags & ERRF_SCAN_TIMEOUT)
+        return report_error(FLUID_ERR_TIMEOUT,
+                            "fluid_selftest_radix_wait: the digit look-back wait gave up, as it should");
+    return FLUID_OK;
+}
+
 extern "C" int32_t fluid_selftest_scan_wait(int32_t device, float *ms) {
     using namespace fcu;
     auto fail = [](cudaError_t e) {

@@ -157,6 +157,7 @@ def lib():
         "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
         "fluid_grid_build_static": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp]),
         "fluid_selftest_scan_wait": (i32, [i32, C.POINTER(C.c_float)]),
+        "fluid_selftest_radix_wait": (i32, [i32, C.POINTER(C.c_float)]),
         "fluid_batch_create": (P, [C.POINTER(FluidSimConfig), u32]),
         "fluid_batch_destroy": (None, [P]),
         "fluid_batch_boxes": (u32, [P]),
@@ -226,6 +227,15 @@ def selftest_scan_wait(device=0):
     returns (status, kernel ms); ERR_TIMEOUT is the expected status."""
     ms = C.c_float(0.0)
     rc = lib().fluid_selftest_scan_wait(device, C.byref(ms))
+    return rc, ms.value
+
+
+def selftest_radix_wait(device=0):
+    """Runs a radix digit pass's bounded look-back out
+    (fluid_selftest_radix_wait): returns (status, kernel ms); ERR_TIMEOUT is
+    the expected status."""
+    ms = C.c_float(0.0)
+    rc = lib().fluid_selftest_radix_wait(device, C.byref(ms))
     return rc, ms.value
 
 

@@ -471,6 +471,13 @@ int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const FluidGrid *
  * the kernel's time. Nothing faults or hangs, and the device stays usable. */
 int32_t fluid_selftest_scan_wait(int32_t device, float *ms);
 
+/* The same for a radix digit pass of the grid build: one block claims the
+ * second tile while the first never publishes its digit counts, so every
+ * digit's bounded look-back (2^20 polls) gives up. FLUID_ERR_TIMEOUT when it
+ * gave up and recorded it, as it should; *ms (if not null) the kernel's
+ * time. Nothing faults or hangs, and the device stays usable. */
+int32_t fluid_selftest_radix_wait(int32_t device, float *ms);
+
 #ifdef __cplusplus
 }
 #endif
