@@ -356,6 +356,7 @@ static_assert(kRadix == kSortThreads, "one thread per digit");
 #ifndef FCU_SORT_MATCH
 #define FCU_SORT_MATCH 0
 #endif
+
 __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
     const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t n, int shift,
     const uint32_t *__restrict__ digit_counts, unsigned long long *tile_status, uint32_t *tile_ctr,
@@ -384,24 +385,31 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
         const uint64_t i = wbase + (uint64_t)r * 32 + lane;
         key[r] = i < n ? __ldg(&keys_in[i]) : 0u;
     }
+    // every round's digit peers first (ballots and registers only), then the
+    // rounds in order: the leader of each group of peers adds the group to
+    // the warp's count of its digit and hands the old count to the group
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
         const bool live = wbase + (uint64_t)r * 32 + lane < n;
-        const uint32_t d = (key[r] >> shift) & (kRadix - 1);
         const uint32_t act = __ballot_sync(0xffffffffu, live);
+        const uint32_t d = (key[r] >> shift) & (kRadix - 1);
 #if FCU_SORT_MATCH
-        const uint32_t peers = live ? __match_any_sync(act, d) : 0u;
+        const uint32_t pe = live ? __match_any_sync(act, d) : 0u;
 #else
-        const uint32_t peers = digit_peers(act, d);
+        const uint32_t pe = digit_peers(act, d);
 #endif
-        rank[r] = 0;
-        if (live) {
-            const uint32_t before = s_hist[warp][d];
-            rank[r] = before + __popc(peers & lt);
-            __syncwarp(act);
-            if (lane == (uint32_t)(__ffs(peers) - 1)) s_hist[warp][d] = before + __popc(peers);
-        }
-        __syncwarp();
+        rank[r] = live ? pe : 0u;  // a live lane is its own peer, so nonzero
+    }
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const uint32_t peers = rank[r];
+        const uint32_t d = (key[r] >> shift) & (kRadix - 1);
+        const uint32_t leader = peers ? (uint32_t)(__ffs(peers) - 1) : lane;
+        uint32_t before = 0;
+        if (peers && lane == leader) before = atomicAdd(&s_hist[warp][d], (uint32_t)__popc(peers));
+        before = __shfl_sync(0xffffffffu, before, leader);
+        rank[r] = before + __popc(peers & lt);
+        __syncwarp();  // this round's adds land before the next round's
     }
     __syncthreads();
     // thread = digit d: the warps' exclusive counts of it, and its tile count
