@@ -131,3 +131,22 @@ def test_grid_every_digit_pass_count(orc, fcu, wl, dims, passes):
     _, e_starts, e_perm = orc.grid_build(og, pos)
     assert np.array_equal(starts, e_starts)
     assert np.array_equal(perm, e_perm)
+
+
+@pytest.mark.parametrize("n", [1, 4095, 4096, 4097, 3 * 4096 + 5])
+def test_grid_of_one_cell_at_tile_boundaries(orc, fcu, n):
+    """Every key equal (one cell): the run of keys spans every tile, so each
+    tile's end of it is a candidate run end and only the last one counts."""
+    g = fcu.FluidGrid()
+    g.min[:] = [0.0, 0.0, 0.0]
+    g.cell = 1.0
+    g.dims[:] = [1, 1, 1]
+    og = orc.OrGrid()
+    og.min[:] = [0.0, 0.0, 0.0]
+    og.cell = 1.0
+    og.dims[:] = [1, 1, 1]
+    pos = np.random.default_rng(n).uniform(-2, 3, (n, 4)).astype(np.float32)
+    starts, perm = fcu.grid_build_host(pos, g)
+    _, e_starts, e_perm = orc.grid_build(og, pos)
+    assert list(starts) == [0, n] and np.array_equal(starts, e_starts)
+    assert np.array_equal(perm, e_perm) and np.array_equal(perm, np.arange(n, dtype=perm.dtype))
