@@ -38,6 +38,10 @@
 #ifndef FCU_MINB_KAPPA
 #define FCU_MINB_KAPPA 0
 #endif
+// The batch's kappa sweeps (box lookups and per-box accumulators) would take
+// 87-88 registers; held to the one box's 80 so that as many threads stay
+// resident (768 a SM).
+constexpr int kBatchKappaThreads = 768;
 #ifndef FCU_STAGE
 #define FCU_STAGE 32
 #endif
@@ -654,7 +658,7 @@ __device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
 // density_div's divergence sums again over the list, with this
 // iteration's velocities.
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB_KAPPA) k_div_kappa(Geo g, SimBufs b, int slot,
+__global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_KAPPA) k_div_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -871,7 +875,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_apply(Geo g, SimBufs b
 
 // ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
+__global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
     const uint32_t n = g.n;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
