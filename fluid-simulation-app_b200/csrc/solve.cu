@@ -29,9 +29,10 @@
 #ifndef FCU_B_N5
 #define FCU_B_N5 1
 #endif
-// Minimum resident blocks per SM that density_div (one box, at 128 threads
-// a block; scaled for other block sizes) and the kappa sweeps are
-// compiled for (0: none), and density_div's hits staged per round.
+// Minimum resident blocks per SM that density_div (at 128 threads a block;
+// scaled for other block sizes; a batch too: its instance measured 3 %
+// faster held to it) and the one box's kappa sweeps are compiled for (0:
+// none), and density_div's hits staged per round.
 #ifndef FCU_MINB_DD
 #define FCU_MINB_DD 7
 #endif
@@ -493,7 +494,7 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
 }
 
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, kB ? 0 : FCU_MINB_DD * 128 / TPB)
+__global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
     k_density_div(const __grid_constant__ Geo g, SimBufs b, int slot) {
     __shared__ uint16_t s_hit[kStage + FCU_DD_CHUNK - 1][TPB];
     __shared__ uint32_t s_beg[9][TPB];
