@@ -1225,6 +1225,27 @@ void or_sim_substep_tol(OrSim *s, const OrStep *st, float div_tol, float den_tol
     integrate(s, *st, 1.0f - std::exp(-LENS_RATE * st->dt));
 }
 
+// One kernel of the substep on the current working set, for the per-kernel
+// checks of the tests (the substep functions above run them in order).
+double or_sim_kernel(OrSim *s, int kernel, const OrStep *st) {
+    const double n = (double)s->n;
+    switch (kernel) {
+    case OR_KERNEL_DENSITY:
+        rebuild(s);
+        return (double)density_div(s, st->dt) / kFixedScale / n;
+    case OR_KERNEL_DIV_APPLY: apply_kappa(s, st->dt, false); return 0.0;
+    case OR_KERNEL_DIV_KAPPA: return (double)div_kappa(s, st->dt) / kFixedScale / n;
+    case OR_KERNEL_FORCES_EVAL: forces_eval(s); return 0.0;
+    case OR_KERNEL_FORCES_APPLY: forces_den_apply(s, *st, step_xsph_blend(s->p, st->dt)); return 0.0;
+    case OR_KERNEL_DEN_KAPPA: return (double)den_kappa(s, st->dt) / kFixedScale / n;
+    case OR_KERNEL_DEN_APPLY: apply_kappa(s, st->dt, true); return 0.0;
+    case OR_KERNEL_INTEGRATE: integrate(s, *st, 1.0f - std::exp(-LENS_RATE * st->dt)); return 0.0;
+    default: return -1.0;
+    }
+}
+
+float or_det_exp(float x) { return or_exp(x); }
+
 // reduce_stats, sim_solve.wgsl:800-874; the compression sum is exact.
 void or_sim_stats(OrSim *s, float out[14]) {
     const OrParams &p = s->p;
@@ -1415,6 +1436,17 @@ void or_sim_field(const OrSim *s, int field, void *out) {
     case OR_FIELD_ACCEL: copy_out(out, s->accel); break;
     case OR_FIELD_XSPH: copy_out(out, s->xsph); break;
     case OR_FIELD_WALL_GRAD: copy_out(out, s->wgrad); break;
+    case OR_FIELD_WORK_PREV_VEL: copy_out(out, s->wpvel); break;
+    case OR_FIELD_WORK_PREV_P: copy_out(out, s->wpp); break;
+    case OR_FIELD_WORK_TEMP: copy_out(out, s->wtemp); break;
+    case OR_FIELD_PINC: copy_out(out, s->pinc); break;
+    case OR_FIELD_NBR: {
+        uint32_t *o = (uint32_t *)out;
+        const uint32_t cap = s->p.nbr_cap;
+        for (size_t i = 0; i < n; ++i)
+            for (uint32_t k = 0; k < cap; ++k) o[i * cap + k] = k < s->nbr_n[i] ? s->nbr[(size_t)k * n + i] : 0xffffffffu;
+        break;
+    }
     case OR_FIELD_COUNTERS: {
         uint32_t *o = (uint32_t *)out;
         o[0] = s->clamp_count;

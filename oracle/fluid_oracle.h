@@ -141,6 +141,24 @@ void or_sim_substep_tol(OrSim *s, const OrStep *st, float div_tol, float den_tol
 void or_sim_get_state64(const OrSim *s, double *pos4, double *vel4);
 /* sizeof the substep's arithmetic type: 4 (the oracle), 8 (the FP64 oracle). */
 int or_sim_real_bytes(void);
+/* One kernel of the substep on the current working set, in isolation (the
+ * per-kernel checks of the tests): DENSITY is the rebuild and density_div;
+ * the kappa kernels return their mean residual, the others 0. */
+enum {
+    OR_KERNEL_DENSITY = 0,
+    OR_KERNEL_DIV_APPLY = 1,
+    OR_KERNEL_DIV_KAPPA = 2,
+    OR_KERNEL_FORCES_EVAL = 3,
+    OR_KERNEL_FORCES_APPLY = 4,
+    OR_KERNEL_DEN_KAPPA = 5,
+    OR_KERNEL_DEN_APPLY = 6,
+    OR_KERNEL_INTEGRATE = 7
+};
+double or_sim_kernel(OrSim *s, int kernel, const OrStep *st);
+/* The per-particle exp of the finger blend (sim_solve.wgsl:122), the
+ * deterministic evaluation the CUDA path shares. */
+float or_det_exp(float x);
+
 /* reduce_stats into out[14] (sim_solve.wgsl:800-874). */
 void or_sim_stats(OrSim *s, float out[14]);
 /* One tracer pass (splat, resolve, advect), sim_tracers.wgsl. */
@@ -161,7 +179,12 @@ enum {
     OR_FIELD_ACCEL = 9,    /* float4[n] */
     OR_FIELD_XSPH = 10,    /* float4[n] */
     OR_FIELD_WALL_GRAD = 11,
-    OR_FIELD_COUNTERS = 12 /* uint32[2]: clamp count, neighbour overflow */
+    OR_FIELD_COUNTERS = 12, /* uint32[2]: clamp count, neighbour overflow */
+    OR_FIELD_WORK_PREV_VEL = 13, /* float4[n], working order */
+    OR_FIELD_WORK_PREV_P = 14,   /* float[n], working order */
+    OR_FIELD_WORK_TEMP = 15,     /* float[n], working order */
+    OR_FIELD_PINC = 16,          /* float[n]: k*rho of the last den_kappa */
+    OR_FIELD_NBR = 17            /* uint32[n][cap]: each particle's list, 0xffffffff past nbr_n */
 };
 void or_sim_field(const OrSim *s, int field, void *out);
 

@@ -14,7 +14,10 @@ LIB_PATH = os.path.join(HERE, "_build", "libfluid_oracle.so")
 LIB64_PATH = os.path.join(HERE, "_build", "libfluid_oracle64.so")
 
 FIELD = dict(density=0, alpha=1, kd=2, pressure=3, nbr_n=4, starts=5, perm=6, work_pos=7,
-             work_vel=8, accel=9, xsph=10, wall_grad=11, counters=12)
+             work_vel=8, accel=9, xsph=10, wall_grad=11, counters=12, work_prev_vel=13,
+             work_prev_p=14, work_temp=15, pinc=16, nbr=17)
+KERNEL = dict(density=0, div_apply=1, div_kappa=2, forces_eval=3, forces_apply=4, den_kappa=5,
+              den_apply=6, integrate=7)
 
 
 class OrGrid(C.Structure):
@@ -121,6 +124,8 @@ def load_library(path):
         "or_field_filter": (None, [f32p, U, U, F, F, f32p]),
         "or_sim_get_state64": (None, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "or_sim_real_bytes": (C.c_int, []),
+        "or_sim_kernel": (D, [C.c_void_p, C.c_int, C.POINTER(OrStep)]),
+        "or_det_exp": (F, [F]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -285,11 +290,18 @@ class Sim:
                       starts=(self.cells + 1, np.uint32), perm=(n, np.uint32),
                       work_pos=((n, 4), np.float32), work_vel=((n, 4), np.float32),
                       accel=((n, 4), np.float32), xsph=((n, 4), np.float32),
-                      wall_grad=((n, 4), np.float32), counters=(2, np.uint32))
+                      wall_grad=((n, 4), np.float32), counters=(2, np.uint32),
+                      work_prev_vel=((n, 4), np.float32), work_prev_p=(n, np.float32),
+                      work_temp=(n, np.float32), pinc=(n, np.float32),
+                      nbr=((n, self.p.nbr_cap), np.uint32))
         shape, dt = shapes[name]
         out = np.zeros(shape, dt)
         self.L.or_sim_field(self.h, FIELD[name], _ptr(out))
         return out
+
+    def kernel(self, name, step):
+        """One kernel of the substep on the working set (or_sim_kernel)."""
+        return self.L.or_sim_kernel(self.h, KERNEL[name], C.byref(step))
 
 
 def set_threads(n):
