@@ -512,6 +512,10 @@ size_t scan_region_bytes(uint32_t len) {
 // The zeroed part of the workspace: the starts scan's look-back region,
 // every pass's tile counter and tile status words, every pass's digit
 // counts.
+__global__ void k_fill_u32(uint32_t *p, uint32_t n, uint32_t v) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) p[i] = v;
+}
+
 struct SortRegion {
     unsigned long long *fill_ctl;
     uint32_t *tile_ctr[kMaxPasses];
@@ -620,8 +624,51 @@ int32_t report_error(int32_t code, const std::string &msg);
 // which tile 0 never publishes, so its look-back polls status[0] until the
 // kSpinLimit bound, records ERRF_SCAN_TIMEOUT and treats the missing prefix
 // as zero. Nothing faults or hangs; the context stays usable.
-// One block of a radix digit pass that claims tile 1 while tile 0 never
-// publishes its digit counts: every digit's bounded look-back gives up. The
+namespace fcu {
+
+int32_t read_build_status(const uint32_t *err, cudaStream_t st, const char *who) {
+    uint32_t flags = 0;
+    cudaError_t e = cudaMemcpyAsync(&flags, err, 4, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return report_error(FLUID_ERR_CUDA, std::string(who) + ": " + cudaGetErrorString(e));
+    if (flags & (ERRF_SCAN_TIMEOUT | ERRF_SORT_TIMEOUT))
+        return report_error(FLUID_ERR_TIMEOUT,
+                            std::string(who) + ": a look-back wait of the build gave up; its starts and "
+                                               "permutation are invalid");
+    return FLUID_OK;
+}
+
+cudaError_t enqueue_stalled_radix_pass(const GridWork &w, cudaStream_t st) {
+    if (w.n < 2 * kSortTile || w.passes < 1) return cudaErrorInvalidValue;
+    const SortRegion r = sort_region(w.scan_ctl, w.n, w.cells, w.passes);
+    cudaError_t e = cudaMemsetAsync(w.scan_ctl, 0, w.scan_ctl_bytes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.k2, 0, 4ull * w.n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(w.err, 0, 4, st);
+    if (e != cudaSuccess) return e;
+    // the tile counter starts at 1, so the one block claims tile 1
+    k_fill_u32<<<1, 32, 0, st>>>(r.tile_ctr[0], 1, 1u);
+    k_radix_pass<<<1, kSortThreads, 0, st>>>(w.k2, nullptr, w.n, 0, r.digit_counts, r.tile_status[0],
+                                             r.tile_ctr[0], w.err, w.k1, w.v1, nullptr, 1u);
+    return cudaGetLastError();
+}
+
+}  // namespace fcu
+
+extern "C" int32_t fluid_grid_build_status(const void *workspace, uint32_t n, const FluidGrid *grid,
+                                           void *stream) {
+    using namespace fcu;
+    if (!grid || !workspace) return report_error(FLUID_ERR_ARG, "fluid_grid_build_status: null argument");
+    const uint64_t cells = (uint64_t)grid->dims[0] * grid->dims[1] * grid->dims[2];
+    if (cells == 0 || cells >= 0xffffffffull)
+        return report_error(FLUID_ERR_ARG, "fluid_grid_build_status: bad grid dims");
+    const GridWork w = grid_work_carve(const_cast<void *>(workspace), n, (uint32_t)cells, nullptr);
+    return read_build_status(w.err, (cudaStream_t)stream, "fluid_grid_build_status");
+}
+
+// The bounded look-back wait of a radix digit pass, run out on purpose on a
+// real build workspace and reported through fluid_grid_build_status, the
+// query a device-pointer caller uses: one block claims tile 1 while tile 0
+// never publishes its digit counts, so every digit's look-back gives up. The
 // keys are all zero, so the give-up offsets still land inside the outputs.
 extern "C" int32_t fluid_selftest_radix_wait(int32_t device, float *ms) {
     using namespace fcu;
@@ -631,52 +678,38 @@ extern "C" int32_t fluid_selftest_radix_wait(int32_t device, float *ms) {
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) return fail(e);
     const uint32_t n = 2 * kSortTile;
-    uint32_t *keys = nullptr, *keys_out = nullptr, *vals_out = nullptr, *counts = nullptr, *ctr = nullptr,
-             *err = nullptr;
-    unsigned long long *status = nullptr;
+    FluidGrid g{};
+    g.cell = 1.0f;
+    g.dims[0] = 16;
+    g.dims[1] = 16;
+    g.dims[2] = 1;
+    const size_t bytes = grid_work_bytes(n, 256u);
+    void *ws = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};
-    uint32_t flags = 0;
     float t = 0.0f;
-    const uint32_t one = 1u;
+    int32_t rc = FLUID_OK;
     do {
-        if ((e = cudaMalloc(&keys, 4ull * n)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&keys_out, 4ull * n)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&vals_out, 4ull * n)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&counts, 4ull * kRadix)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&status, 8ull * kRadix * 2)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&ctr, 4)) != cudaSuccess) break;
-        if ((e = cudaMalloc(&err, 4)) != cudaSuccess) break;
-        if ((e = cudaMemset(keys, 0, 4ull * n)) != cudaSuccess) break;
-        if ((e = cudaMemset(counts, 0, 4ull * kRadix)) != cudaSuccess) break;
-        if ((e = cudaMemset(status, 0, 8ull * kRadix * 2)) != cudaSuccess) break;
-        if ((e = cudaMemset(err, 0, 4)) != cudaSuccess) break;
-        if ((e = cudaMemcpy(ctr, &one, 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((e = cudaMalloc(&ws, bytes)) != cudaSuccess) break;
         if ((e = cudaEventCreate(&ev[0])) != cudaSuccess) break;
         if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) break;
+        const GridWork w = grid_work_carve(ws, n, 256u, nullptr);
         cudaEventRecord(ev[0]);
-        k_radix_pass<<<1, kSortThreads>>>(keys, nullptr, n, 0, counts, status, ctr, err, keys_out, vals_out,
-                                          nullptr, 1u);
+        if ((e = enqueue_stalled_radix_pass(w, nullptr)) != cudaSuccess) break;
         cudaEventRecord(ev[1]);
         if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) break;
-        if ((e = cudaGetLastError()) != cudaSuccess) break;
         cudaEventElapsedTime(&t, ev[0], ev[1]);
-        if ((e = cudaMemcpy(&flags, err, 4, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+        rc = fluid_grid_build_status(ws, n, &g, nullptr);
     } while (false);
     for (cudaEvent_t x : ev)
         if (x) cudaEventDestroy(x);
-    cudaFree(keys);
-    cudaFree(keys_out);
-    cudaFree(vals_out);
-    cudaFree(counts);
-    cudaFree(status);
-    cudaFree(ctr);
-    cudaFree(err);
+    cudaFree(ws);
     if (e != cudaSuccess) return fail(e);
     if (ms) *ms = t;
-    if (flags & ERRF_SCAN_TIMEOUT)
+    if (rc == FLUID_ERR_TIMEOUT)
         return report_error(FLUID_ERR_TIMEOUT,
-                            "fluid_selftest_radix_wait: the digit look-back wait gave up, as it should");
-    return FLUID_OK;
+                            "fluid_selftest_radix_wait: the digit look-back wait gave up, as it should, "
+                            "and fluid_grid_build_status reported it");
+    return rc;
 }
 
 extern "C" int32_t fluid_selftest_scan_wait(int32_t device, float *ms) {

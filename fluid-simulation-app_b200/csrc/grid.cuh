@@ -56,6 +56,14 @@ size_t grid_work_bytes(uint32_t n, uint32_t cells);
 // Carves `ws` (at least grid_work_bytes) into a GridWork.
 GridWork grid_work_carve(void *ws, uint32_t n, uint32_t cells, uint32_t *err);
 
+// Reads a build's error word on `stream` (waiting for it): FLUID_OK, or
+// FLUID_ERR_TIMEOUT with a reason when a bounded look-back wait gave up.
+int32_t read_build_status(const uint32_t *err, cudaStream_t stream, const char *who);
+// Enqueues one block of a radix digit pass on the scratch of `w` (carved for
+// at least two tiles of keys) that claims tile 1 while tile 0 never
+// publishes: its bounded look-back waits give up and set w.err.
+cudaError_t enqueue_stalled_radix_pass(const GridWork &w, cudaStream_t stream);
+
 // A batch of boxes sharing one grid: slot i belongs to box box_of[i], whose
 // cells are keys cell_base[b] .. cell_base[b] + its cells - 1 (the boxes'
 // cell ranges laid end to end, in box order).

@@ -25,6 +25,12 @@
 // the scans and the error word. Everything else in the scratch is written
 // before it is read.
 //
+// Errors: the build's error word sits at a fixed place, the first 256 bytes
+// of the scratch, and the rest is carved for the build behind it. A look-
+// back wait that gives up sets it; fluid_grid_build_static_status reads it
+// back (after the build, before the next call on the device clears it), so
+// a caller learns that its starts and permutation are invalid.
+//
 // Races: there is ONE scratch area per device. Two calls whose work overlaps
 // on the device (different streams, or different host threads, with no
 // stream order or event between them) share it and corrupt each other's
@@ -45,6 +51,12 @@ namespace {
 // 2^20 positions over 2^18 cells 17.3 MiB (refused).
 constexpr size_t kStaticScratchBytes = (size_t)FLUID_GRID_STATIC_SCRATCH_BYTES;
 static __device__ __align__(256) unsigned char g_scratch[kStaticScratchBytes];
+
+// The error word's slot at the head of the scratch. grid_work_bytes counts
+// 256 bytes for an error word of the workspace's own, which a build with
+// its word elsewhere leaves unused, so the carve behind the slot still
+// ends within grid_work_bytes.
+constexpr size_t kErrBytes = 256;
 
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
@@ -103,7 +115,8 @@ extern "C" int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const 
         return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static: cudaGetSymbolAddress: ") +
                                                 cudaGetErrorString(e));
     cudaStream_t st = (cudaStream_t)stream;
-    GridWork w = grid_work_carve(ws, n, (uint32_t)cells, nullptr);
+    GridWork w = grid_work_carve(static_cast<char *>(ws) + kErrBytes, n, (uint32_t)cells,
+                                 static_cast<uint32_t *>(ws));
     e = cudaMemsetAsync(w.err, 0, 4, st);
     // Without a caller buffer the keys live in k2: pass 0 reads them and
     // writes k1, and k2 is next written by pass 1, after they are consumed.
@@ -119,4 +132,62 @@ extern "C" int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const 
     if (e != cudaSuccess)
         return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static: ") + cudaGetErrorString(e));
     return FLUID_OK;
+}
+
+// The error word of the last fluid_grid_build_static on the current device.
+extern "C" int32_t fluid_grid_build_static_status(void *stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static_status: cudaGetDevice: ") +
+                                                cudaGetErrorString(e));
+    if (dev < 0 || dev >= kMaxDevices)
+        return report_error(FLUID_ERR_ARG, "fluid_grid_build_static_status: device ordinal above 63");
+    void *ws = nullptr;
+    e = scratch_address(dev, &ws);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_grid_build_static_status: cudaGetSymbolAddress: ") +
+                                                cudaGetErrorString(e));
+    return read_build_status(static_cast<const uint32_t *>(ws), (cudaStream_t)stream,
+                             "fluid_grid_build_static_status");
+}
+
+// A radix digit pass's bounded look-back run out on the fixed scratch, as a
+// build of fluid_grid_build_static lays it out, and reported through
+// fluid_grid_build_static_status. Allocates nothing.
+extern "C" int32_t fluid_selftest_static_radix_wait(int32_t device, float *ms) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_selftest_static_radix_wait: ") + cudaGetErrorString(e));
+    if (device < 0 || device >= kMaxDevices)
+        return report_error(FLUID_ERR_ARG, "fluid_selftest_static_radix_wait: device ordinal above 63");
+    void *ws = nullptr;
+    e = scratch_address(device, &ws);
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    float t = 0.0f;
+    int32_t rc = FLUID_OK;
+    do {
+        if (e != cudaSuccess) break;
+        if ((e = cudaEventCreate(&ev[0])) != cudaSuccess) break;
+        if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) break;
+        const uint32_t n = 2 * kSortTile;
+        const GridWork w = grid_work_carve(static_cast<char *>(ws) + kErrBytes, n, 256u,
+                                           static_cast<uint32_t *>(ws));
+        cudaEventRecord(ev[0]);
+        if ((e = enqueue_stalled_radix_pass(w, nullptr)) != cudaSuccess) break;
+        cudaEventRecord(ev[1]);
+        if ((e = cudaEventSynchronize(ev[1])) != cudaSuccess) break;
+        cudaEventElapsedTime(&t, ev[0], ev[1]);
+        rc = fluid_grid_build_static_status(nullptr);
+    } while (false);
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    if (e != cudaSuccess)
+        return report_error(FLUID_ERR_CUDA, std::string("fluid_selftest_static_radix_wait: ") + cudaGetErrorString(e));
+    if (ms) *ms = t;
+    if (rc == FLUID_ERR_TIMEOUT)
+        return report_error(FLUID_ERR_TIMEOUT,
+                            "fluid_selftest_static_radix_wait: the digit look-back wait gave up, as it should, "
+                            "and fluid_grid_build_static_status reported it");
+    return rc;
 }

@@ -156,6 +156,9 @@ def lib():
         "fluid_grid_build": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp, u64, vp]),
         "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
         "fluid_grid_build_static": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp]),
+        "fluid_grid_build_status": (i32, [vp, u32, C.POINTER(FluidGrid), vp]),
+        "fluid_grid_build_static_status": (i32, [vp]),
+        "fluid_selftest_static_radix_wait": (i32, [i32, C.POINTER(C.c_float)]),
         "fluid_selftest_scan_wait": (i32, [i32, C.POINTER(C.c_float)]),
         "fluid_selftest_radix_wait": (i32, [i32, C.POINTER(C.c_float)]),
         "fluid_batch_create": (P, [C.POINTER(FluidSimConfig), u32]),
@@ -236,6 +239,14 @@ def selftest_radix_wait(device=0):
     the expected status."""
     ms = C.c_float(0.0)
     rc = lib().fluid_selftest_radix_wait(device, C.byref(ms))
+    return rc, ms.value
+
+
+def selftest_static_radix_wait(device=0):
+    """The same stalled digit pass on fluid_grid_build_static's fixed
+    scratch, read back through fluid_grid_build_static_status."""
+    ms = C.c_float(0.0)
+    rc = lib().fluid_selftest_static_radix_wait(device, C.byref(ms))
     return rc, ms.value
 
 
@@ -636,6 +647,14 @@ def grid_build_device(pos4_ptr, n, grid, keys_ptr, starts_ptr, perm_ptr, ws_ptr,
                                         C.c_void_p(starts_ptr), C.c_void_p(perm_ptr),
                                         C.c_void_p(ws_ptr), ws_bytes,
                                         C.c_void_p(stream) if stream else None), "grid_build")
+
+
+def grid_build_status(ws_ptr, n, grid, stream=None):
+    """fluid_grid_build_status: the status code of the last build on the
+    workspace (OK, or ERR_TIMEOUT when its starts and permutation are
+    invalid). Not raised, returned."""
+    return lib().fluid_grid_build_status(C.c_void_p(ws_ptr), n, C.byref(grid),
+                                         C.c_void_p(stream) if stream else None)
 
 
 def grid_workspace_bytes(n, grid):

@@ -443,6 +443,17 @@ int32_t fluid_grid_build(const float *pos4, uint32_t n, const FluidGrid *grid, u
                          uint32_t *starts, uint32_t *perm, void *workspace, uint64_t ws_bytes,
                          void *stream);
 
+/* Whether the fluid_grid_build last run on `workspace` (with the same n and
+ * grid) completed: FLUID_OK, or FLUID_ERR_TIMEOUT (reason in
+ * fluid_last_error()) when one of its bounded look-back waits gave up, in
+ * which case its starts and permutation are invalid (a missing prefix was
+ * counted as zero, so slots may repeat). Reads the build's error word on
+ * `stream` after the work queued there and waits for it; allocates nothing.
+ * Follows the reference's convention that a failure carries its reason
+ * (crates/fluid-ffi/src/lib.rs:86-108). */
+int32_t fluid_grid_build_status(const void *workspace, uint32_t n, const FluidGrid *grid,
+                                void *stream);
+
 /* The same from and to host memory (allocates, copies, synchronises). */
 int32_t fluid_grid_build_host(const float *pos4, uint32_t n, const FluidGrid *grid,
                               uint32_t *starts, uint32_t *perm);
@@ -464,6 +475,13 @@ int32_t fluid_grid_build_host(const float *pos4, uint32_t n, const FluidGrid *gr
 int32_t fluid_grid_build_static(const float *pos4, uint32_t n, const FluidGrid *grid,
                                 uint32_t *keys, uint32_t *starts, uint32_t *perm, void *stream);
 
+/* Whether the last fluid_grid_build_static on the current device completed:
+ * FLUID_OK, or FLUID_ERR_TIMEOUT when a bounded look-back wait gave up and
+ * its starts and permutation are invalid. The error word lives in the fixed
+ * scratch, so read it after that build and before the next call on the
+ * device, which clears it. Reads on `stream` and waits; allocates nothing. */
+int32_t fluid_grid_build_static_status(void *stream);
+
 /* Failure detection, exercised (no counterpart in the reference): runs one
  * block of the grid's look-back scan whose predecessor never publishes, so
  * the scan's bounded wait (2^20 polls) gives up. Returns FLUID_ERR_TIMEOUT
@@ -475,8 +493,16 @@ int32_t fluid_selftest_scan_wait(int32_t device, float *ms);
  * second tile while the first never publishes its digit counts, so every
  * digit's bounded look-back (2^20 polls) gives up. FLUID_ERR_TIMEOUT when it
  * gave up and recorded it, as it should; *ms (if not null) the kernel's
- * time. Nothing faults or hangs, and the device stays usable. */
+ * time. The give-up is read back through fluid_grid_build_status on the
+ * workspace the pass ran on. Nothing faults or hangs, and the device stays
+ * usable. */
 int32_t fluid_selftest_radix_wait(int32_t device, float *ms);
+
+/* The same stalled digit pass on fluid_grid_build_static's fixed scratch,
+ * laid out as its builds lay it out, reported through
+ * fluid_grid_build_static_status: FLUID_ERR_TIMEOUT, as it should.
+ * Allocates nothing. */
+int32_t fluid_selftest_static_radix_wait(int32_t device, float *ms);
 
 #ifdef __cplusplus
 }

@@ -79,6 +79,10 @@ def test_static_build_matches_workspace_build_twice(fcu, n, dims):
                 _static_build(fcu, d_pos.data_ptr(), n, g, with_keys, starts.data_ptr(),
                               perm.data_ptr(), stream.cuda_stream)
             stream.synchronize()
+            if name == "workspace":
+                assert fcu.grid_build_status(base, n, g, stream.cuda_stream) == 0
+            else:
+                assert fcu.lib().fluid_grid_build_static_status(C.c_void_p(stream.cuda_stream)) == 0
             out[name] = (keys.cpu().numpy()[:n], starts.cpu().numpy(), perm.cpu().numpy()[:n])
         for a, b in zip(out["workspace"], out["static"]):
             assert np.array_equal(a, b)
