@@ -62,13 +62,27 @@ SUBSTEPS_PER_FRAME = 4
 ALGO_BYTES = {"grid": 20.0, "gather": 116.0, "density_div": 44.0, "div_kappa": 28.0,
               "div_apply": 36.0, "forces_eval": 84.0, "forces_den_apply": 92.0,
               "den_kappa": 36.0, "den_apply": 36.0, "integrate": 120.0}
-# DRAM bytes (read + write) per particle per launch, from ncu captures of
-# each kernel on this workload at its full 1,048,576 particles
-# (profiles/list_sweeps_tilt_1m.md, profiles/density_div_tilt_1m.md).
+# DRAM bytes (read + write) per particle per launch: a constant taken from
+# one ncu capture of each kernel on this workload at its full 1,048,576
+# particles (dram__bytes_read.sum + dram__bytes_write.sum), not measured by
+# this script; a kernel change calls for a new capture.
 NCU_TRAFFIC_PER_PARTICLE = {"den_kappa": (583.2e6 + 19.4e6) / 1048576,
                             "den_apply": (604.1e6 + 15.5e6) / 1048576,
                             "div_apply": (604.1e6 + 15.5e6) / 1048576,
                             "density_div": (71.9e6 + 505.6e6) / 1048576}
+
+
+def workload_config(w, n):
+    """The workload both arms run, as the JSON line's `config`."""
+    return {"workload": WORKLOAD, "particles": n, "lattice": "x".join(str(v) for v in w["lattice"]),
+            "box_m": "x".join(str(v) for v in w["box_hi"]), "spacing_m": w["spacing"], "h_ratio": 1.2,
+            "tracers": w["tracers"], "frame_dt_s": float(np.float32(1.0 / 120.0)),
+            "step": "one 1/120 s frame: 4 DFSPH substeps (substeps_for's floor at 5 mm), "
+                    "reduce_stats, one tracer pass; the metric counts substeps",
+            "substeps_per_frame": SUBSTEPS_PER_FRAME,
+            "solve": "tolerance div 1% / den 0.1%, cap 100, FP64 residuals",
+            "tilt": "seed 1, three sinusoids per axis, <= 35 degrees, 0.2-2 Hz",
+            "l2": "working set > 126 MB L2; no flush"}
 
 
 def load(name, path):
@@ -328,26 +342,16 @@ def cuda_arm(args):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "particles": n, "lattice": list(w["lattice"]),
-                       "box_m": list(w["box_hi"]), "spacing_m": w["spacing"], "h_ratio": 1.2,
-                       "tracers": w["tracers"], "frame_dt_s": dt,
-                       "step": "one DFSPH substep; 4 per 1/120 s frame (substeps_for's floor at 5 mm)",
-                       "substeps": substeps, "substeps_per_frame": substeps / args.steps,
-                       "solve": "tolerance div 1% / den 0.1%, cap 100, FP64 residuals",
-                       "mean_div_iters": div_it / max(substeps, 1),
-                       "mean_den_iters": den_it / max(substeps, 1),
-                       "parallelism": f"replicas x{world}" if world > 1 else "single box",
-                       "l2": "working set ~0.5 GB > 126 MB L2; no flush"},
-            "density_error": {"compression_avg": final.compression_avg,
-                              "compression_max": final.compression_max,
-                              "den_residual_last": final.den_residual,
-                              "clamps": final.clamp_count},
+            "config": workload_config(w, n),
             "particle_frames_per_s": n * world * args.steps / (ms_max / 1000.0),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 160 * e2e_sub / args.steps,
                     "d2h_bytes_per_step": 64 + 64 + 64},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None if traffic is None else traffic * n,
+                         "traffic_source": "constant from one ncu capture of this kernel on this "
+                                           "workload (dram__bytes_read.sum + dram__bytes_write.sum), "
+                                           "not measured in this run",
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic": "own records, list-free (36 B per particle for the kappa sweeps)",
                          "mean_neighbours": mean_nbrs,
@@ -363,6 +367,15 @@ def cuda_arm(args):
             "batched": batched,
             "adjoint": adjoint,
             "grid": grid,
+            # last, so that the end of the line shows them
+            "solve": {"substeps": substeps, "mean_div_iters": div_it / max(substeps, 1),
+                      "mean_den_iters": den_it / max(substeps, 1),
+                      "parallelism": f"replicas x{world}" if world > 1 else "single box"},
+            "density_error": {"compression_avg": final.compression_avg,
+                              "compression_max": final.compression_max,
+                              "den_residual_last": after.den_residual,
+                              "clamps_per_particle_substep": (after.clamp_count - before.clamp_count)
+                              / float(n * max(substeps, 1))},
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -571,6 +584,15 @@ def adjoint_leg(args, fcu, wl, world, local):
     g, gx = adj.backward()
     _, bwd_ms = adj.timing()
     n = adj.n
+    # the same forward and backward in FP64 on the same frozen schedule: its
+    # gradient stays finite over the whole horizon where FP32 overflows
+    a64 = fcu.Adjoint(cfg, ADJ_FRAMES, SUBSTEPS_PER_FRAME, dt, vc, ADJ_CHECKPOINT, precision=64)
+    a64.set_schedule(div_it, den_it)
+    loss64 = a64.forward(forces, 0.01, target)
+    g64, gx64 = a64.backward()
+    f64_ms, b64_ms = a64.timing()
+    a64.close()
+    gv64 = np.concatenate([g64.ravel(), [gx64]])
     adj.close()
     # the production step on the same box, same substeps
     sim = fcu.Sim(cfg)
@@ -598,6 +620,9 @@ def adjoint_leg(args, fcu, wl, world, local):
             "backward_over_production_forward": bwd_ms / prod_ms,
             "mean_div_iters": float(div_it.mean()), "mean_den_iters": float(den_it.mean()),
             "grad_norm": float(np.linalg.norm(gv)) if np.all(np.isfinite(gv)) else None,
+            "fp64": {"loss": loss64, "forward_ms": f64_ms, "backward_ms": b64_ms,
+                     "grad_norm": float(np.linalg.norm(gv64)) if np.all(np.isfinite(gv64)) else None,
+                     "grad_xsph": float(gx64)},
             "grad_note": "sensitivities grow exponentially with the horizon on this splashing "
                          "workload; the gradient is checked against FP64 central differences "
                          "on short horizons (tests/test_gpu_adjoint.py)"}
@@ -660,49 +685,70 @@ def cpu_sample(fcu, sim, dt):
 
 
 def reference_arm(args):
-    """The CPU oracle as the reference implementation, all host threads."""
+    """The reference implementation on the host: the CPU oracle (this
+    project's restatement of the reference's WGSL step, which exists only as
+    shaders) on the same workload, the same frames and the same count as the
+    CUDA arm: tilt_1m's 1,048,576-particle lattice and 4,096 tracers seeded
+    as fluid_sim_create seeds them, `warmup` untimed frames, then `steps`
+    timed frames, each four tolerance-solve substeps, reduce_stats and a
+    tracer pass, with the same seeded tilt. All host threads (OpenMP)."""
     world, rank, local = dist_init()
     if rank != 0:
         return
     sys.path.insert(0, ROOT)
     from oracle import oracle as orc
     wl = load("workloads", os.path.join(PKG, "workloads.py"))
-    # A bounded sample per step: one substep of a 32x16x32 block of the same
-    # lattice, spacing and physics (the 1M box's corner), so K + W steps stay
-    # within minutes on the host.
-    lattice = [32, 16, 32]
-    spacing = 0.005
+    w = wl.WORKLOADS[WORKLOAD]
+    lattice, spacing = list(w["lattice"]), w["spacing"]
     pos = orc.seed_block([0, 0, 0], spacing, lattice, 0.005, 1)
-    p = orc.params_box([0, 0, 0], [0.32, 0.16, 0.32], spacing, 1.2, 1000.0, len(pos))
+    n = len(pos)
+    p = orc.params_box([0, 0, 0], list(w["box_hi"]), spacing, 1.2, 1000.0, n)
     p.xsph_blend = 0.01
-    o = orc.Sim(p, 0)
+    o = orc.Sim(p, w["tracers"])
     o.set_state(pos4=pos)
-    dt = float(np.float32(1.0 / 120.0) / np.float32(4.0))
-    forces = wl.tilt_schedule(1, args.warmup + args.steps, 1.0 / 120.0)
-    vc = float(np.float32(0.4) * np.float32(spacing) / np.float32(dt))
+    size = [float(np.float32(x) * np.float32(spacing)) for x in lattice]
+    o.set_tracers(orc.seed_tracers_box(w["tracers"], [0, 0, 0], size, p))
+    frames = args.warmup + args.steps
+    forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
+    dt = float(np.float32(1.0 / 120.0))
+    dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
+    vc = float(np.float32(0.4) * np.float32(spacing) / np.float32(dts))
+    iters = np.zeros(2, np.int64)
 
-    def one(k):
-        f = forces[k]
-        o.substep_tol(orc.make_step(force=tuple(float(x) for x in f), dt=dt, v_clamp=vc), 0.01,
-                      0.001, 100)
+    def frame(k):
+        f = tuple(float(x) for x in forces[k])
+        st = orc.make_step(force=f, dt=dts, v_clamp=vc)
+        for _ in range(SUBSTEPS_PER_FRAME):
+            it, _ = o.substep_tol(st, 0.01, 0.001, 100)
+            iters[:] += it
+        o.stats()
+        o.tracer_pass(orc.make_step(force=f, dt=dt, seed=k))
 
     for k in range(args.warmup):
-        one(k)
+        frame(k)
+    iters[:] = 0
     t0 = time.perf_counter()
-    for k in range(args.warmup, args.warmup + args.steps):
-        one(k)
+    for k in range(args.warmup, frames):
+        frame(k)
     t = time.perf_counter() - t0
-    value = len(pos) * args.steps / t
+    final = o.stats()
+    substeps = SUBSTEPS_PER_FRAME * args.steps
+    value = n * substeps / t
     cores = os.cpu_count()
     print(json.dumps({
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000.0 * t / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "sample": "32x16x32 block of the tilt_1m lattice"},
+        "config": workload_config(w, n),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"one substep of a {len(pos)}-particle block per step"},
+                         "sample": f"the whole workload: {args.steps} frames of {n} particles "
+                                   f"({substeps} substeps) after {args.warmup} warm-up frames, "
+                                   f"OpenMP over {cores} threads, {t:.1f} s"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "solve": {"substeps": substeps, "mean_div_iters": float(iters[0]) / substeps,
+                  "mean_den_iters": float(iters[1]) / substeps},
+        "density_error": {"compression_avg": float(final[0]), "compression_max": float(final[1])},
     }), flush=True)
 
 

@@ -31,6 +31,7 @@
 // reversed.
 //
 // The reference has no adjoint; nothing here replaces a reference call.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -80,10 +81,51 @@ template <class T> DEV T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + 
 template <class T> DEV V3<T> zero3() { return mk(T(0), T(0), T(0)); }
 template <class T> DEV T comp(V3<T> a, int k) { return k == 0 ? a.x : (k == 1 ? a.y : a.z); }
 
-template <class T> DEV void atomic_add3(V3<T> *p, V3<T> v) {
-    atomicAdd(&p->x, v.x);
-    atomicAdd(&p->y, v.y);
-    atomicAdd(&p->z, v.z);
+// Fixed-order sums: each block adds its threads' four values by xor-shuffle
+// trees in every warp, then thread q adds the warps' totals in warp order
+// into part[4 * block + q]; k_sum_parts adds the blocks' partials in a fixed
+// order. No floating-point atomics, so the sums are the same bits on every
+// run (for a given launch shape).
+DEV void block_sums4(double (&v)[4], double *part) {
+    __shared__ double s[32][4];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+    }
+    if (lane == 0)
+        for (int q = 0; q < 4; ++q) s[warp][q] = v[q];
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (uint32_t w = 0; w < nw; ++w) t += s[w][threadIdx.x];
+        part[4 * (size_t)blockIdx.x + threadIdx.x] = t;
+    }
+}
+
+// Where the four sums of k_sum_parts go (null: dropped); `add` adds them to
+// what is there instead of overwriting it.
+struct Sum4Out {
+    double *dst[4];
+    int add;
+};
+
+__global__ void __launch_bounds__(256) k_sum_parts(const double *__restrict__ part, uint32_t nb, Sum4Out o) {
+    __shared__ double s[256];
+    for (int q = 0; q < 4; ++q) {
+        if (!o.dst[q]) continue;
+        double t = 0.0;
+        for (uint32_t b = threadIdx.x; b < nb; b += 256) t += part[4 * (size_t)b + q];
+        s[threadIdx.x] = t;
+        __syncthreads();
+        for (uint32_t w = 128; w > 0; w >>= 1) {
+            if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) *o.dst[q] = (o.add ? *o.dst[q] : 0.0) + s[0];
+        __syncthreads();
+    }
 }
 
 // Value and three partial derivatives (forward mode over a position).
@@ -602,7 +644,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_kappa(MP<T> p, uint32_t n, in
                                                          const uint32_t *__restrict__ nbr, const T *__restrict__ gsl,
                                                          const uint32_t *__restrict__ nbr_n, const T *__restrict__ rho,
                                                          const T *__restrict__ alpha, const V3<T> *__restrict__ wg,
-                                                         T *kd, T *pinc, double *res) {
+                                                         T *kd, T *pinc, unsigned long long *res) {
     const LaneOf L = lane_of(n);
     const uint32_t i = L.i;
     double term = 0.0;
@@ -624,9 +666,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_kappa(MP<T> p, uint32_t n, in
         }
     }
     if (res) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) term += __shfl_xor_sync(0xffffffffu, term, o);
-        if ((threadIdx.x & 31) == 0 && term != 0.0) atomicAdd(res, term);
+        // the production solve's exact sum: 2^-28 units added as integers
+        const unsigned long long q = warp_sum_u64(fixed_term(term));
+        if ((threadIdx.x & 31) == 0 && q) atomicAdd(res, q);
     }
 }
 
@@ -757,7 +799,7 @@ __global__ void __launch_bounds__(256) k_m_integrate(MP<T> p, uint32_t n, T dt, 
 // The loss sums: centre of mass and squared density deviation.
 template <class T>
 __global__ void __launch_bounds__(256) k_m_loss(MP<T> p, uint32_t n, const V3<T> *__restrict__ x,
-                                                const T *__restrict__ rho, double *acc) {
+                                                const T *__restrict__ rho, double *part) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     double s[4] = {0.0, 0.0, 0.0, 0.0};
     if (i < n) {
@@ -767,12 +809,7 @@ __global__ void __launch_bounds__(256) k_m_loss(MP<T> p, uint32_t n, const V3<T>
         const double d = (double)rho[i] / (double)p.rho0 - 1.0;
         s[3] = d * d;
     }
-    for (int q = 0; q < 4; ++q) {
-        double t = s[q];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd(&acc[q], t);
-    }
+    block_sums4(s, part);
 }
 
 // ---- reverse kernels -------------------------------------------------------------
@@ -949,7 +986,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_
                                                                 const uint32_t *__restrict__ nbr_n,
                                                                 const T *__restrict__ kd, const V3<T> *__restrict__ wg,
                                                                 const V3<T> *__restrict__ vbar, V3<T> *abar, V3<T> *bbar,
-                                                                T *kdbar, V3<T> *xbar, double *fbar, double *cbar) {
+                                                                T *kdbar, V3<T> *xbar, double *part) {
     const LaneOf L = lane_of(n);
     const uint32_t i = L.i;
     double red[4] = {0.0, 0.0, 0.0, 0.0};
@@ -982,12 +1019,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_r_forces_apply(MP<T> p, uint32_
         const J3<T> J = wall_grad_jac(p, xi);
         xbar[i] = xbar[i] + xs + (-dt * kdi) * jt_mul(J, vb);
     }
-    for (int q = 0; q < 4; ++q) {
-        double t = red[q];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-        if ((threadIdx.x & 31) == 0 && t != 0.0) atomicAdd(q < 3 ? &fbar[q] : cbar, t);
-    }
+    block_sums4(red, part);
 }
 
 // One pair's share of forces_eval in particle a's equation (neighbour b,
@@ -1333,7 +1365,9 @@ struct AdjImpl : AdjBase {
     Tape<T> fin;  // the final density pass of the loss
     T *kd = nullptr, *pinc = nullptr, *pressure = nullptr;
     T *gsl = nullptr;  // the substep's gradient scales beside its list (forward sweeps only)
-    double *acc = nullptr;  // residual (1), loss sums (4)
+    double *acc = nullptr;  // loss sums (4)
+    unsigned long long *res_acc = nullptr;  // a loop's residual, 2^-28 fixed point
+    double *part = nullptr;  // per-block partial sums of the fixed-order reductions
     // controls of the last forward
     std::vector<double> forces;
     double xsph = 0.0, target[3] = {0, 0, 0}, com[3] = {0, 0, 0};
@@ -1447,6 +1481,8 @@ struct AdjImpl : AdjBase {
         AK(alloc(&pinc, N));
         AK(alloc(&pressure, N));
         AK(alloc(&acc, 8));
+        AK(alloc(&res_acc, 1));
+        AK(alloc(&part, 4 * (size_t)std::max(nblk(n * kLanes, kAdjThreads), nblk(n, 256))));
         AK(alloc(&xbar, N));
         AK(alloc(&vbar, N));
         AK(alloc(&xbar2, N));
@@ -1511,9 +1547,10 @@ struct AdjImpl : AdjBase {
     }
 
     int32_t read_residual(double *r) {
-        AK(cudaMemcpyAsync(r, acc, 8, cudaMemcpyDeviceToHost, stream));
+        unsigned long long q = 0;
+        AK(cudaMemcpyAsync(&q, res_acc, 8, cudaMemcpyDeviceToHost, stream));
         AK(cudaStreamSynchronize(stream));
-        *r /= (double)n;
+        *r = (double)q / kFixedScale / (double)n;
         return FLUID_OK;
     }
 
@@ -1533,8 +1570,8 @@ struct AdjImpl : AdjBase {
                                                       t.rho, t.rhon, t.alpha, t.wg, over);
         // divergence loop
         uint32_t nd = decide ? 0u : div_it[k];
-        if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
-        double *res = decide ? acc : nullptr;
+        if (decide) AK(cudaMemsetAsync(res_acc, 0, 8, stream));
+        unsigned long long *res = decide ? res_acc : nullptr;
         k_m_kappa<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[0], t.nbr, gsl, t.nbr_n, t.rho, t.alpha,
                                                     t.wg, t.kddiv.empty() ? kd : t.kddiv[0], nullptr, res);
         uint32_t it = 0;
@@ -1553,7 +1590,7 @@ struct AdjImpl : AdjBase {
                                                         kd_t, t.wg, nullptr, nullptr);
             ++it;
             if (decide || it < nd) {
-                if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
+                if (decide) AK(cudaMemsetAsync(res_acc, 0, 8, stream));
                 k_m_kappa<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, 0, dt, t.x, t.vdiv[it], t.nbr, gsl, t.nbr_n, t.rho,
                                                             t.alpha, t.wg, t.kddiv[it], nullptr, res);
             }
@@ -1569,7 +1606,7 @@ struct AdjImpl : AdjBase {
         it = 0;
         for (;;) {
             if (!decide && it >= ne) break;
-            if (decide) AK(cudaMemsetAsync(acc, 0, 8, stream));
+            if (decide) AK(cudaMemsetAsync(res_acc, 0, 8, stream));
             k_m_kappa<T><<<BL, kAdjThreads, 0, stream>>>(mp, n, 1, dt, t.x, t.vden[it], t.nbr, gsl, t.nbr_n, t.rho,
                                                         t.alpha, t.wg, t.kdden[it], pinc, res);
             if (decide) {
@@ -1641,8 +1678,8 @@ struct AdjImpl : AdjBase {
         }
         rc = density(x, fin);
         if (rc != FLUID_OK) return rc;
-        AK(cudaMemsetAsync(acc + 1, 0, 32, stream));
-        k_m_loss<T><<<nblk(n, 256), 256, 0, stream>>>(mp, n, x, fin.rho, acc + 1);
+        k_m_loss<T><<<nblk(n, 256), 256, 0, stream>>>(mp, n, x, fin.rho, part);
+        k_sum_parts<<<1, 256, 0, stream>>>(part, nblk(n, 256), Sum4Out{{acc + 1, acc + 2, acc + 3, acc + 4}, 0});
         AK(cudaEventRecord(e1, stream));
         double sums[4];
         AK(cudaMemcpyAsync(sums, acc + 1, 32, cudaMemcpyDeviceToHost, stream));
@@ -1707,8 +1744,9 @@ struct AdjImpl : AdjBase {
                                                           xbar);
         }
         k_r_forces_apply<T><<<B, kAdjThreads, 0, stream>>>(mp, n, dt, T(xsph), t.x, t.blend, t.nbr, t.nbr_n, t.kdf,
-                                                           t.wg, vbar, abar, bbar, kdbar, xbar, fbar + 3 * (size_t)k,
-                                                           cbar);
+                                                           t.wg, vbar, abar, bbar, kdbar, xbar, part);
+        double *fk = fbar + 3 * (size_t)k;
+        k_sum_parts<<<1, 256, 0, stream>>>(part, B, Sum4Out{{fk, fk + 1, fk + 2, cbar}, 1});
         k_r_forces_eval<T><<<B, kAdjThreads, 0, stream>>>(mp, n, t.x, t.vdiv[nd], t.nbr, t.nbr_n, t.rho, t.rhon,
                                                           t.pp, abar, bbar, kdbar, pbar, xbar, vbar, rhobar, rhonbar,
                                                           ppbar);

@@ -461,6 +461,19 @@ void or_seed_tracers(uint32_t count, const float extent[2], float fill, uint32_t
     }
 }
 
+// The box geometry's tracers (sim.rs:105-122 moved to a box): uniform over
+// the region [lo, lo + size) from the same hash stream, stored relative to
+// the tracer box centre and packed over its half extent e.
+void or_seed_tracers_box(uint32_t count, const float lo[3], const float size[3], const float centre[3],
+                         const float e[2], uint32_t *out2) {
+    auto unit = [](uint32_t h) { return (float)h / 4294967295.0f; };
+    for (uint32_t i = 0; i < count; ++i) {
+        float rel[3];
+        for (int a = 0; a < 3; ++a) rel[a] = lo[a] + unit(or_hash(i * 3 + a)) * size[a] - centre[a];
+        or_pack_tracer(rel, 0.0f, e, out2 + 2 * (size_t)i);
+    }
+}
+
 // sim.rs:215-252
 void or_pack_step(const float force[3], const float omega[3], const float domega[3], float dt,
                   float v_clamp, uint32_t seed, uint32_t touch_n, float touch_r,

@@ -82,6 +82,10 @@ float or_wall_adhesion(float t);
 void or_lattice_dims(float spacing, const float extent[2], float fill, uint32_t out[3]);
 uint32_t or_seed_slab(float spacing, const float extent[2], float fill, float *out4);
 void or_seed_tracers(uint32_t count, const float extent[2], float fill, uint32_t *out2);
+/* Tracers of a box: uniform over [lo, lo + size), relative to centre,
+ * packed over the half extent e (the same hash stream as the slab's). */
+void or_seed_tracers_box(uint32_t count, const float lo[3], const float size[3], const float centre[3],
+                         const float e[2], uint32_t *out2);
 uint16_t or_half_bits(float x);
 float or_half_value(uint16_t bits);
 void or_pack_tracer(const float pos[3], float speed, const float extent[2], uint32_t out[2]);

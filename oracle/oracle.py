@@ -98,6 +98,7 @@ def load_library(path):
         "or_seed_slab": (U, [F, f32p, F, C.c_void_p]),
         "or_seed_tracers": (None, [U, f32p, F, u32p]),
         "or_seed_block": (U, [f32p, F, u32p, F, C.c_uint64, C.c_void_p]),
+        "or_seed_tracers_box": (None, [U, f32p, f32p, f32p, f32p, u32p]),
         "or_pack_tracer": (None, [f32p, F, f32p, u32p]),
         "or_unpack_tracer": (None, [u32p, f32p, f32p]),
         "or_pack_step": (None, [f32p, f32p, f32p, F, F, U, U, F, C.c_void_p,
@@ -202,6 +203,14 @@ def seed_block(lo, spacing, dims, jitter, seed):
     out = np.zeros((n, 4), np.float32)
     lib().or_seed_block(f32(lo), spacing, u32(dims), jitter, seed, _ptr(out))
     return out
+
+
+def seed_tracers_box(count, lo, size, params):
+    """Packed tracers uniform over [lo, lo + size) of a box (params_box)."""
+    out = np.zeros(2 * count, np.uint32)
+    e = f32([params.tracer_e[0], params.tracer_e[1]])
+    lib().or_seed_tracers_box(count, f32(lo), f32(size), f32(list(params.tracer_c)), e, out)
+    return out.reshape(-1, 2)
 
 
 def params_slab(extent, spacing, h_ratio, count):
