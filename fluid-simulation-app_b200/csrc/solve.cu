@@ -54,6 +54,11 @@ constexpr int kBatchKappaThreads = 768;
 #ifndef FCU_DD_CHUNK
 #define FCU_DD_CHUNK 4
 #endif
+// FCU_TILED_KAPPA > 0: the one-box den_kappa runs list-free, cell-tiled
+// (k_den_kappa_tiled) with that many cells per tile.
+#ifndef FCU_TILED_KAPPA
+#define FCU_TILED_KAPPA 0
+#endif
 #ifndef FCU_MINB
 #define FCU_MINB 0
 #endif
@@ -313,6 +318,48 @@ __device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, 
 #endif
 }
 
+#if FCU_GRAD_LIST
+// The same walk over the gradient list: each entry carries the pair's
+// kernel gradient itself (slot in w), `use(gradient, record)`.
+__device__ __forceinline__ float4 glist_ld(const float4 *p) {
+#if FCU_LIST_CS
+    return __ldcs(p);
+#else
+    return __ldg(p);
+#endif
+}
+template <int B, class T, class Load, class Use>
+__device__ __forceinline__ void walk_grad(const float4 *__restrict__ nbr, uint32_t n, uint32_t i,
+                                          uint32_t cnt, Load load, Use use) {
+    float4 e[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+        e[u] = ((uint32_t)u < cnt) ? glist_ld(&nbr[(size_t)u * n + i]) : make_float4(0.f, 0.f, 0.f, __uint_as_float(i));
+    for (uint32_t k = 0; k < cnt; k += B) {
+        T v[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) v[u] = load(__float_as_uint(e[u].w));
+        float4 en[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            en[u] = (k + B + u < cnt) ? glist_ld(&nbr[(size_t)(k + B + u) * n + i])
+                                      : make_float4(0.f, 0.f, 0.f, __uint_as_float(i));
+#if FCU_L2PF
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const uint32_t kf = k + B * (1 + FCU_L2PF) + u;
+            if (kf < cnt) prefetch_l2(&nbr[(size_t)kf * n + i]);
+        }
+#endif
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (k + u < cnt) use(f3(e[u].x, e[u].y, e[u].z), v[u]);
+#pragma unroll
+        for (int u = 0; u < B; ++u) e[u] = en[u];
+    }
+}
+#endif
+
 struct PosKd {
     float4 p;
     float kd;
@@ -439,14 +486,14 @@ struct DensitySums {
 
 template <class KP>
 __device__ __forceinline__ float density_pair(const KP &P, DensitySums &d, F3 pos, F3 vel,
-                                              F3 x, float r2, float4 vj) {
+                                              F3 x, float r2, float4 vj, F3 &gw) {
     const float r = sqrtf(r2);
     const float q = r * P.inv_h;
     d.w_sum += kernel_q(P, q);
     const float wn = fmaxf(1.0f - q, 0.0f);
     d.rho_near += wn * wn * wn;
     const float gs = grad_scale(P, r, q);
-    const F3 gw = gs * x;
+    gw = gs * x;
     d.grad_sum = d.grad_sum + gw;
     d.grad_sq += dot(gw, gw);
     d.drho += dot(vel - xyz(vj), gw);
@@ -485,8 +532,14 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
                 const F3 x = pos - xyz(__ldg(&b.wpos[k]));
                 const float r2 = dot(x, x);
                 if (r2 >= P.support_sq) continue;
-                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
-                if (found < P.nbr_cap) b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
+                F3 gw;
+                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]), gw);
+                if (found < P.nbr_cap) {
+                    b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
+#if FCU_GRAD_LIST
+                    b.nbr_g[(size_t)found * n + i] = make_float4(gw.x, gw.y, gw.z, __uint_as_float(k));
+#endif
+                }
                 found++;
             }
         }
@@ -603,9 +656,16 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
                     for (int u = 0; u < kP2; ++u) {
                         if (h + u < staged) {
                             const F3 x = pos - xyz(pj[u]);
-                            const float gs = density_pair(K, d, pos, vel, x, dot(x, x), vj[u]);
+                            F3 gw;
+                            const float gs = density_pair(K, d, pos, vel, x, dot(x, x), vj[u], gw);
                             const uint32_t idx = found + h + u;
-                            if (idx < cap) b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
+                            if (idx < cap) {
+                                b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
+#if FCU_GRAD_LIST
+                                b.nbr_g[(size_t)idx * n + i] =
+                                    make_float4(gw.x, gw.y, gw.z, __uint_as_float(j[u]));
+#endif
+                            }
                         }
                     }
                 }
@@ -704,12 +764,10 @@ __device__ __forceinline__ F3 kappa_sum(const SimBufs &b, uint32_t i, uint32_t n
 // ---- apply_kappa_wide: div_apply / den_apply (sim_solve.wgsl:608-621) -----
 // For the density iterations the applied pressure k*rho that den_kappa held
 // back joins the pressure here, with the kappa it belongs to.
-template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure,
-                                                                   int gate) {
+template <bool kB>
+__device__ __forceinline__ void apply_at(const Geo &g, const SimBufs &b, uint32_t i, int add_pressure,
+                                         int gate) {
     const uint32_t n = g.n;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
     const uint32_t bi = box_index<kB>(g, i);
     if (gated_out<kB>(g, bi, gate)) return;
     const float mass = params_of<kB>(g, bi).mass;
@@ -724,6 +782,12 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int a
     if (add_pressure) b.pressure[i] += b.pinc[i];
 }
 
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure, int gate) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < g.n) apply_at<kB>(g, b, i, add_pressure, gate);
+}
+
 // ---- forces_eval (sim_solve.wgsl:524-592) ---------------------------------
 // With kDiv, the same walk also forms the divergence prediction of
 // k_div_kappa (the same pair terms, in the same order, so the same sums):
@@ -732,10 +796,9 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int a
 // schedule runs this after each divergence apply, so the prediction that
 // only decides whether the loop stops costs no sweep of its own.
 template <bool kB, bool kDiv>
-__device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b, int slot, int gate) {
+__device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b, uint32_t i, bool live,
+                                                 int slot, int gate) {
     const uint32_t n = g.n;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
     if (!kDiv && !live) return;
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
@@ -818,11 +881,13 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
 
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
-    forces_eval_body<kB, false>(g, b, slot, gate);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    forces_eval_body<kB, false>(g, b, i, i < g.n, slot, gate);
 }
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
-    forces_eval_body<kB, true>(g, b, slot, gate);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    forces_eval_body<kB, true>(g, b, i, i < g.n, slot, gate);
 }
 
 // fingers (sim_solve.wgsl:103-127)
@@ -875,12 +940,10 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_apply(Geo g, SimBufs b
 }
 
 // ---- den_kappa (sim_solve.wgsl:674-698) ------------------------------------
-template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
-                                                                       int gate) {
+template <bool kB>
+__device__ __forceinline__ void den_kappa_at(const Geo &g, const SimBufs &b, uint32_t i, bool live, int slot,
+                                             int gate) {
     const uint32_t n = g.n;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = i < n;
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
     if (live && !gated_out<kB>(g, bi, gate)) {
@@ -891,10 +954,16 @@ __global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
         float drho = 0.0f;
+#if FCU_GRAD_LIST
+        walk_grad<FCU_B_PV, float4>(
+            b.nbr_g, n, i, cnt, [&](uint32_t j) { return __ldg(&b.wvel[j]); },
+            [&](F3 gw, const float4 &v) { drho += dot(vel - xyz(v), gw); });
+#else
         walk<FCU_B_PV, PosVel>(
             b.nbr, n, i, cnt,
             [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
             [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
+#endif
         const float rho = __ldg(&b.density[i]);
         drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;
@@ -906,6 +975,193 @@ __global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_
         term = fixed_term((double)rho_star / (double)rho0 - 1.0);
     }
     add_term<kB>(&g.solve[bi].acc_den[slot], term);
+}
+
+template <bool kB, int TPB>
+__global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
+                                                                       int gate) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    den_kappa_at<kB>(g, b, i, i < g.n, slot, gate);
+}
+
+// ---- the batch's loop sweeps over a work list -------------------------------
+// Inside a tolerance loop only the boxes whose loop goes on are swept. The
+// loop's finishing kernel lists them (k_tol_finish: each active box with the
+// exclusive prefix of its tiles of kListTile consecutive slots), and these
+// persistent kernels walk that list: block after block takes the next tile,
+// finds its box by binary search over the prefix, and runs the same
+// per-slot body as the one-launch-per-sweep kernels. Boxes that stopped cost
+// nothing; the sums are those of the gated kernels, slot for slot.
+constexpr uint32_t kListTile = kSolveThreads;
+
+// Slot of this thread in work item w of list `which`; false for a lane past
+// its box's last slot (i is then that last slot).
+__device__ __forceinline__ bool work_slot(const Geo &g, int which, uint32_t nact, uint32_t w, uint32_t &i) {
+    const uint32_t *pre = g.wl_prefix[which];
+    uint32_t lo = 0, hi = nact;
+    while (hi - lo > 1u) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (pre[mid] <= w) lo = mid;
+        else hi = mid;
+    }
+    const uint32_t bx = g.wl_box[which][lo];
+    const uint32_t first = g.first[bx], cnt = g.box[bx].count;
+    i = first + (w - pre[lo]) * kListTile + threadIdx.x;
+    const bool live = i < first + cnt;
+    if (!live) i = first + cnt - 1u;
+    return live;
+}
+
+__global__ void __launch_bounds__(kListTile, kBatchKappaThreads / kListTile) k_apply_list(Geo g, SimBufs b,
+                                                                                       int add_pressure, int which) {
+    const uint32_t nact = *g.wl_nact[which];
+    const uint32_t total = nact ? g.wl_prefix[which][nact] : 0u;
+    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+        uint32_t i;
+        if (work_slot(g, which, nact, w, i)) apply_at<true>(g, b, i, add_pressure, kGateNone);
+    }
+}
+
+__global__ void __launch_bounds__(kListTile, kBatchKappaThreads / kListTile) k_den_kappa_list(Geo g, SimBufs b,
+                                                                                           int slot, int which) {
+    const uint32_t nact = *g.wl_nact[which];
+    const uint32_t total = nact ? g.wl_prefix[which][nact] : 0u;
+    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+        uint32_t i;
+        const bool live = work_slot(g, which, nact, w, i);
+        den_kappa_at<true>(g, b, i, live, slot, kGateNone);
+    }
+}
+
+__global__ void __launch_bounds__(kListTile, FCU_MINB) k_forces_div_list(Geo g, SimBufs b, int slot, int which) {
+    const uint32_t nact = *g.wl_nact[which];
+    const uint32_t total = nact ? g.wl_prefix[which][nact] : 0u;
+    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
+        uint32_t i;
+        const bool live = work_slot(g, which, nact, w, i);
+        forces_eval_body<true, true>(g, b, i, live, slot, kGateNone);
+    }
+}
+
+// ---- den_kappa without the list, cell-tiled ----------------------------------
+// The same prediction as k_den_kappa with no neighbour list: each CTA takes
+// grid rows (y, z) in turn and walks a row in tiles of T x-adjacent cells.
+// A tile's particles draw their neighbours from nine slot ranges, one per
+// stencil row (oz, oy), each covering cells x0 - 1 .. x0 + T; those ranges'
+// positions and velocities are staged in shared memory with 128-bit loads,
+// once per tile. Each thread then tests its particle's 27-cell candidates in
+// stencil order (rows by oz then oy, slots ascending: the order density_div
+// found them in), r^2 < support^2 and not itself, stops after the list cap,
+// and sums the same pair terms with the gradient scale recomputed exactly as
+// density_div formed it (IEEE square root and division), so the sum is the
+// list walk's sum bit for bit. A tile whose neighbourhood does not fit the
+// staging area takes the list walk.
+template <int TPB, int T, int CAP>
+__global__ void __launch_bounds__(TPB) k_den_kappa_tiled(Geo g, SimBufs b, int slot) {
+    __shared__ float4 s_pos[CAP];
+    __shared__ float4 s_vel[CAP];
+    __shared__ uint32_t s_st[9][T + 3];  // starts of cells x0-1 .. x0+T+1 per stencil row (clamped)
+    __shared__ uint32_t s_off[9];        // shared index of each row's first staged slot
+    __shared__ uint32_t s_lo[9];         // global slot of each row's first staged slot
+    __shared__ uint32_t s_total;
+    const DevParams &P = g.one;
+    const uint32_t n = g.n, dx = P.dims[0], dy = P.dims[1], dz = P.dims[2];
+    const uint32_t rows = dy * dz, cap = P.nbr_cap;
+    const float mass = P.mass, rho0 = P.rho0, dt = g.st[0].s.dt;
+    unsigned long long term = 0;
+    for (uint32_t row = blockIdx.x; row < rows; row += gridDim.x) {
+        const uint32_t y = row % dy, z = row / dy;
+        const uint32_t rbase = row * dx;
+        if (__ldg(&b.starts[rbase]) == __ldg(&b.starts[rbase + dx])) continue;  // uniform: empty row
+        for (uint32_t x0 = 0; x0 < dx; x0 += T) {
+            const uint32_t x1 = x0 + T < dx ? x0 + T : dx;  // tile cells x0 .. x1 - 1
+            const uint32_t p0 = __ldg(&b.starts[rbase + x0]), p1 = __ldg(&b.starts[rbase + x1]);
+            if (p0 == p1) continue;
+            __syncthreads();  // the previous tile's staging is no longer read
+            if (threadIdx.x < 9u * (T + 3)) {
+                const uint32_t r = threadIdx.x / (T + 3), k = threadIdx.x % (T + 3);
+                const int cz = (int)z + (int)(r / 3) - 1, cy = (int)y + (int)(r % 3) - 1;
+                const int cx = (int)x0 - 1 + (int)k;
+                uint32_t v = 0;
+                if (cz >= 0 && cz < (int)dz && cy >= 0 && cy < (int)dy) {
+                    const uint32_t rb = ((uint32_t)cz * dy + (uint32_t)cy) * dx;
+                    const int c = cx < 0 ? 0 : (cx > (int)dx ? (int)dx : cx);
+                    v = __ldg(&b.starts[rb + (uint32_t)c]);
+                }
+                s_st[r][k] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                uint32_t tot = 0;
+                for (int r = 0; r < 9; ++r) {
+                    // staged: cells max(x0-1, 0) .. min(x1, dx-1)
+                    const uint32_t a = s_st[r][x0 == 0 ? 1 : 0];
+                    const uint32_t e = s_st[r][(x1 < dx ? x1 : dx - 1) - x0 + 2];
+                    s_lo[r] = a;
+                    s_off[r] = tot;
+                    tot += e - a;
+                }
+                s_total = tot;
+            }
+            __syncthreads();
+            const uint32_t total = s_total;
+            const bool staged = total <= (uint32_t)CAP;
+            if (staged) {
+                for (int r = 0; r < 9; ++r) {
+                    const uint32_t a = s_lo[r], o = s_off[r];
+                    const uint32_t m = (r < 8 ? s_off[r + 1] : total) - o;
+                    for (uint32_t k = threadIdx.x; k < m; k += TPB) {
+                        s_pos[o + k] = __ldg(&b.wpos[a + k]);
+                        s_vel[o + k] = __ldg(&b.wvel[a + k]);
+                    }
+                }
+            }
+            __syncthreads();
+            for (uint32_t i = p0 + threadIdx.x; i < p1; i += TPB) {
+                const F3 pos = xyz(__ldg(&b.wpos[i]));
+                const F3 vel = xyz(__ldg(&b.wvel[i]));
+                float drho = 0.0f;
+                if (staged) {
+                    const uint32_t bx = axis_cell(pos.x, P.box_min[0], P.cell, dx);
+                    const uint32_t kx0 = bx > 0 ? bx - x0 : 1u;                      // cell max(bx-1, 0)
+                    const uint32_t kx1 = (bx + 1 < dx ? bx + 1 : dx - 1) - x0 + 2;  // cell min(bx+1, dx-1) + 1
+                    uint32_t found = 0;
+                    for (int r = 0; r < 9 && found < cap; ++r) {
+                        const uint32_t a = s_st[r][kx0], e = s_st[r][kx1];
+                        const int32_t sh = (int32_t)s_off[r] - (int32_t)s_lo[r];
+                        for (uint32_t j = a; j < e; ++j) {
+                            if (j == i) continue;
+                            const float4 pj = s_pos[(uint32_t)((int32_t)j + sh)];
+                            const F3 x = pos - xyz(pj);
+                            const float r2 = dot(x, x);
+                            if (r2 >= P.support_sq) continue;
+                            const float rr = sqrtf(r2);
+                            const float gs = grad_scale(P, rr, rr * P.inv_h);
+                            const float4 vj = s_vel[(uint32_t)((int32_t)j + sh)];
+                            drho += dot(vel - xyz(vj), gs * x);
+                            if (++found >= cap) break;
+                        }
+                    }
+                } else {
+                    walk<FCU_B_PV, PosVel>(
+                        b.nbr, n, i, __ldg(&b.nbr_n[i]),
+                        [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
+                        [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
+                }
+                const float rho = __ldg(&b.density[i]);
+                drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
+                const float rho_star = rho + dt * drho;
+                const float kk = fmaxf(rho_star - rho0, 0.0f) * __ldg(&b.alpha[i]) / (dt * dt);
+                const float kdv = kk / rho;
+                b.kd[i] = kdv;
+                b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
+                b.pinc[i] = kk * rho;
+                term += fixed_term((double)rho_star / (double)rho0 - 1.0);
+            }
+        }
+    }
+    // one integer add per thread that summed anything: order-free
+    if (term) atomicAdd(&g.solve[0].acc_den[slot], term);
 }
 
 // ---- integrate (sim_solve.wgsl:709-756) ------------------------------------
@@ -1006,6 +1262,60 @@ __global__ void __launch_bounds__(256) k_tol_finish(Geo g, int which, int first,
     }
     any = __syncthreads_or(any);
     if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
+    if (!g.wl_box[which]) return;
+    // the work list of the loop's next iteration: active boxes in box order
+    // with the exclusive prefix of their tiles (a block scan per chunk)
+    __shared__ uint32_t s_wc[8], s_wt[8];
+    __shared__ uint32_t s_carry_c, s_carry_t;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (threadIdx.x == 0) {
+        s_carry_c = 0u;
+        s_carry_t = 0u;
+    }
+    __syncthreads();
+    for (uint32_t base = 0; base < g.nboxes; base += blockDim.x) {
+        const uint32_t bx = base + threadIdx.x;
+        uint32_t act = 0, til = 0;
+        if (bx < g.nboxes) {
+            const DevSolve &sv = g.solve[bx];
+            act = (which == 0 ? sv.div_active : sv.den_active) ? 1u : 0u;
+            til = act ? (g.box[bx].count + kListTile - 1u) / kListTile : 0u;
+        }
+        uint32_t c = act, t = til;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t cu = __shfl_up_sync(0xffffffffu, c, o), tu = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= (uint32_t)o) {
+                c += cu;
+                t += tu;
+            }
+        }
+        if (lane == 31) {
+            s_wc[warp] = c;
+            s_wt[warp] = t;
+        }
+        __syncthreads();
+        uint32_t oc = s_carry_c, ot = s_carry_t;
+        for (uint32_t w = 0; w < warp; ++w) {
+            oc += s_wc[w];
+            ot += s_wt[w];
+        }
+        if (act) {
+            g.wl_box[which][oc + c - 1u] = bx;
+            g.wl_prefix[which][oc + c - 1u] = ot + t - til;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (uint32_t w = 0; w < nw; ++w) {
+                s_carry_c += s_wc[w];
+                s_carry_t += s_wt[w];
+            }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        g.wl_prefix[which][s_carry_c] = s_carry_t;
+        *g.wl_nact[which] = s_carry_c;
+    }
 }
 
 // ---- reduce_stats (sim_solve.wgsl:800-874) ---------------------------------
@@ -1311,7 +1621,33 @@ void launch_forces_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot,
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b) {
     FCU_SWEEP(k_forces_apply, kTuneForcesApply, kSolveThreads, g, b);
 }
+void launch_den_kappa_tiled(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int cells_per_tile) {
+    if (!g.n || g.box_of) return;
+    const uint32_t rows = g.one.dims[1] * g.one.dims[2];
+    const uint32_t grid = rows < 148u * 8u ? rows : 148u * 8u;
+    if (cells_per_tile <= 2) k_den_kappa_tiled<128, 2, 512><<<grid, 128, 0, s>>>(g, b, slot);
+    else if (cells_per_tile <= 4) k_den_kappa_tiled<128, 4, 768><<<grid, 128, 0, s>>>(g, b, slot);
+    else k_den_kappa_tiled<128, 8, 1280><<<grid, 128, 0, s>>>(g, b, slot);
+}
+// The persistent loop sweeps over a batch's work list: a fixed grid (the
+// list's length is only known on the device) of kListTile-thread blocks.
+constexpr uint32_t kListBlocks = 148u * 6u;
+void launch_apply_list(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int which) {
+    k_apply_list<<<kListBlocks, kListTile, 0, s>>>(g, b, add_pressure ? 1 : 0, which);
+}
+void launch_den_kappa_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which) {
+    k_den_kappa_list<<<kListBlocks, kListTile, 0, s>>>(g, b, slot, which);
+}
+void launch_forces_div_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which) {
+    k_forces_div_list<<<kListBlocks, kListTile, 0, s>>>(g, b, slot, which);
+}
 void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
+#if FCU_TILED_KAPPA
+    if (!g.box_of) {
+        launch_den_kappa_tiled(s, g, b, slot, FCU_TILED_KAPPA);
+        return;
+    }
+#endif
     FCU_SWEEP(k_den_kappa, kTuneDenKappa, kSolveThreads, g, b, slot, gate);
 }
 void launch_integrate(cudaStream_t s, const Geo &g, const SimBufs &b, int div_slot, int den_slot,
