@@ -17,6 +17,12 @@ pieces.
 Tolerance: a float32 sum of ~56 pair terms against its float64 value, so
 each component within 1e-4 of the sum of its terms' magnitudes (the
 reference's density check allows 1e-3 of the value).
+
+The tracer pass (splat, resolve, advect with respawns, sim_tracers.wgsl:
+54-183) is restated the same way over three frames of 4,096 tracers: the
+branch decisions (respawn draws) compared in float32 as the shader does,
+positions to within one step of the unorm16 packing, depth and charge to
+within the float16 packing.
 """
 import json
 import math
@@ -334,3 +340,129 @@ def test_the_deterministic_exp_is_within_two_ulp_of_exp(orc):
     assert worst <= 2.0, worst
     assert L.or_det_exp(0.0) == 1.0
     assert L.or_det_exp(-100.0) == 0.0
+
+
+# ---- the tracer pass (sim_tracers.wgsl:54-183), restated -------------------
+FIXED = 65536.0
+TAU, TAU_STRAY, T_CHARGE = 3.0, 0.25, 4.0
+M32 = 0xFFFFFFFF
+
+
+def pcg(x):
+    h = (x * 747796405 + 2891336453) & M32
+    h = (((h >> ((h >> 28) + 4)) ^ h) * 277803737) & M32
+    return ((h >> 22) ^ h) & M32
+
+
+def i32_trunc(v):
+    """WGSL i32(f32): toward zero, saturating."""
+    return int(max(min(math.trunc(v), 2 ** 31 - 1), -2 ** 31))
+
+
+def tracer_pass_np(p, pos, vel, tracers, dt, seed):
+    """splat -> resolve -> advect for the slab geometry (box extent
+    -(box_min + cell)), in float64 except where the shader compares float32
+    values to decide a branch. Returns decoded (x, y, z, charge) per tracer
+    and which tracers respawned."""
+    bmin = np.array(list(p.box_min), np.float64)
+    cell = float(np.float32(p.cell))
+    dims = np.array(list(p.dims), np.int64)
+    e = -(bmin + cell)
+    grid = np.zeros((dims[2], dims[1], dims[0], 4), np.int64)
+    for k in range(len(pos)):
+        u = np.floor(np.maximum((pos[k, :3] - bmin) / cell, 0.0)).astype(np.int64)
+        c = np.minimum(u, dims - 1)
+        g = grid[c[2], c[1], c[0]]
+        for a in range(3):
+            g[a] += i32_trunc(float(np.float32(np.float32(vel[k, a]) * np.float32(FIXED))))
+        g[3] += 1
+    f32 = np.float32
+    thr = f32(f32(dt) / f32(TAU))
+    thr_stray = f32(f32(dt) / f32(TAU_STRAY))
+    out = np.zeros((len(tracers), 4))
+    respawned = np.zeros(len(tracers), bool)
+
+    def respawn(slot, r):
+        r1 = pcg(r)
+        r2 = pcg(r1)
+        r3 = pcg(r2)
+        r4 = pcg(r3)
+        jit = (np.array([r2 >> 20, r3 >> 20, r4 >> 20], np.float64) / 4096.0 - 0.5) * (cell * 0.5)
+        j = r1 % len(pos)
+        q = np.clip(pos[j, :3] + jit, -e, e)
+        out[slot] = [q[0], q[1], q[2], np.linalg.norm(vel[j, :3])]
+        respawned[slot] = True
+
+    for i in range(len(tracers)):
+        r0 = pcg(i ^ pcg(seed))
+        if f32(f32(r0) / f32(4294967295.0)) < thr:
+            respawn(i, r0)
+            continue
+        t = tracers[i]
+        xy = ((np.array([t[0] & 0xFFFF, t[0] >> 16]) / 65535.0) * 2.0 - 1.0) * e[:2]
+        z = float(np.array([t[1] & 0xFFFF], np.uint16).view(np.float16)[0])
+        s = float(np.array([t[1] >> 16], np.uint16).view(np.float16)[0])
+        q = np.array([xy[0], xy[1], z])
+        gp = (q - bmin) / cell - 0.5
+        base = np.clip(np.floor(gp).astype(np.int64), 0, dims - 2)
+        fr = np.clip(gp - base, 0.0, 1.0)
+        mom = np.zeros(3)
+        wc = 0.0
+        for k in range(8):
+            o = np.array([k & 1, (k >> 1) & 1, (k >> 2) & 1])
+            w = np.where(o == 1, fr, 1.0 - fr)
+            wt = w[0] * w[1] * w[2]
+            c = base + o
+            cellv = grid[c[2], c[1], c[0]]
+            mom += wt * cellv[:3]
+            wc += wt * cellv[3]
+        if wc > 0.0:
+            v = mom / (wc * FIXED)
+        elif f32(f32(pcg(r0 ^ 0x85EBCA6B)) / f32(4294967295.0)) < thr_stray:
+            respawn(i, pcg(r0 ^ 0x632BE59B))
+            continue
+        else:
+            v = np.zeros(3)
+        q = np.clip(q + v * dt, -e, e)
+        out[i] = [q[0], q[1], q[2], max(np.linalg.norm(v), s * math.exp(-dt / T_CHARGE))]
+    return out, respawned
+
+
+def decode(orc, tracers, e):
+    out = np.zeros((len(tracers), 4), np.float32)
+    ext = np.ascontiguousarray(e[:2], np.float32)
+    for i, t in enumerate(tracers):
+        orc.lib().or_unpack_tracer(np.ascontiguousarray(t, np.uint32), ext, out[i])
+    return out
+
+
+def test_the_tracer_pass_matches_an_independent_restatement(orc, moving_box):
+    s, b, st = moving_box
+    p = s.p
+    n_tr = 4096
+    t0 = np.zeros((n_tr, 2), np.uint32)
+    orc.lib().or_seed_tracers(n_tr, orc.f32(TB["extent"]), 0.5, t0.reshape(-1))
+    tr = orc.Sim(p, n_tr)
+    rest = s.state()
+    tr.set_state(rest["pos"], rest["vel"], rest["prev_vel"], rest["prev_p"], rest["temp"], rest["id"])
+    tr.set_tracers(t0)
+    dt = float(np.float32(1.0 / 120.0))
+    bmin = np.array(list(p.box_min), np.float64)
+    e = -(bmin + float(np.float32(p.cell)))
+    pos64, vel64 = rest["pos"].astype(np.float64), rest["vel"].astype(np.float64)
+    before = t0.copy()
+    for frame in range(3):
+        seed = 11 + frame
+        want, resp = tracer_pass_np(p, pos64, vel64, before, dt, seed)
+        tr.tracer_pass(orc.make_step(dt=dt, seed=seed))
+        got_raw = tr.tracers()
+        got = decode(orc, got_raw, e)
+        quantum = 2.0 * e[:2] / 65535.0
+        assert np.all(np.abs(got[:, :2] - want[:, :2]) <= 1.01 * quantum), frame
+        z_tol = np.maximum(np.abs(want[:, 2]) * 2.0 ** -10, 2.0 ** -24) * 1.01
+        assert np.all(np.abs(got[:, 2] - want[:, 2]) <= z_tol), frame
+        c_tol = np.maximum(np.abs(want[:, 3]) * 2.0 ** -10, 2.0 ** -24) * 1.01
+        assert np.all(np.abs(got[:, 3] - want[:, 3]) <= c_tol), frame
+        moved = np.linalg.norm(got[:, :3] - decode(orc, before, e)[:, :3], axis=1)
+        assert resp.sum() > 0 and np.count_nonzero(moved[~resp]) > n_tr // 4, frame
+        before = got_raw
