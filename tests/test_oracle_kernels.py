@@ -466,3 +466,31 @@ def test_the_tracer_pass_matches_an_independent_restatement(orc, moving_box):
         moved = np.linalg.norm(got[:, :3] - decode(orc, before, e)[:, :3], axis=1)
         assert resp.sum() > 0 and np.count_nonzero(moved[~resp]) > n_tr // 4, frame
         before = got_raw
+
+
+# reduce_stats (sim_solve.wgsl:758-874) restated over the resting set and the
+# last sweep's densities: the mean compression is a sum (float64 here, an
+# exact fixed-point sum in the oracle), every other slot a min or max, which
+# no summation order changes.
+def test_the_stats_block_matches_an_independent_restatement(orc, moving_box):
+    s, b, st = moving_box
+    s.substep(st)
+    got = s.stats()
+    rho = np.asarray(s.field("density"), np.float64)
+    rest = s.state()
+    c = rho / b.rho0 - 1.0
+    speed = np.linalg.norm(rest["vel"][:, :3].astype(np.float64), axis=1)
+    want = np.array([np.maximum(c, 0.0).mean(), max(c.max(), 0.0), rho.min(), rho.max(),
+                     rest["prev_vel"][:, 3].min(), rest["prev_vel"][:, 3].max(), speed.max(),
+                     rest["temp"].min(), rest["temp"].max(), np.nan, np.nan, speed.min(),
+                     rest["vel"][:, 3].min(), rest["vel"][:, 3].max()])
+    for k in range(14):
+        if k in (9, 10):
+            continue
+        tol = 1e-6 * abs(want[k]) + (1e-9 if k == 0 else 0.0)
+        if k in (6, 11):  # float32 length against float64
+            tol = 1e-6 * abs(want[k]) + 1e-12
+        assert abs(float(got[k]) - want[k]) <= tol, (k, got[k], want[k])
+    counters = s.field("counters")
+    assert got[9] == np.float32(counters[0]) and got[10] == np.float32(counters[1])
+    assert got[0] > 0 and got[6] > 0
