@@ -396,7 +396,7 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     statistics are summed across ranks at the end."""
     import torch
     sharding = load("sharding", os.path.join(PKG, "sharding.py"))
-    cfgs_all = wl.batched_boxes(fcu)
+    cfgs_all = wl.batched_boxes(fcu, nboxes=args.boxes)
     counts = [c.block[0] * c.block[1] * c.block[2] for c in cfgs_all]
     mine = sharding.lpt_shards(counts, world)[rank]
     cfgs = [cfgs_all[b] for b in mine]
@@ -454,7 +454,7 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
             "mean_div_iters_per_box": float(rows[:, 1].mean() / sub),
             "compression_avg_mean": float(rows[:, 2].mean()),
             "compression_avg_worst_box": float(rows[:, 2].max()),
-            "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu,
+            "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu if plain_per_gpu else None,
             "vs_the_same_boxes_as_plain_sims": plain_boxes,
             "autotuned_blocks": chosen,
             "autotune_ms_by_block": {str(t): dict(zip(fcu.Batch.TUNED, [round(float(x), 4) for x in tune_ms[c]]))
@@ -767,12 +767,27 @@ def main():
                     help="skip stepping the batched boxes as separate plain sims")
     ap.add_argument("--profile-substeps", type=int, default=0,
                     help="after the warm-up, run this many substeps as direct launches timed per kernel, then exit")
+    ap.add_argument("--boxes", type=int, default=256,
+                    help="boxes of the batched leg (256: the batched workload; fewer for profiling runs)")
+    ap.add_argument("--batch-only", action="store_true",
+                    help="run the batched leg alone and print it (profiling runs)")
+    ap.add_argument("--adjoint-only", action="store_true",
+                    help="run the adjoint leg alone and print it (profiling runs)")
     ap.add_argument("--grid-only", action="store_true",
                     help="run the 16.7M-position grid leg alone and print it (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
-    if args.grid_only:
+    if args.batch_only or args.adjoint_only:
+        import torch
+        torch.cuda.set_device(0)
+        fcu = load("fluidcu", os.path.join(PKG, "fluidcu.py"))
+        wl = load("workloads", os.path.join(PKG, "workloads.py"))
+        if args.batch_only:
+            print(json.dumps(batched_leg(args, fcu, wl, 1, 0, 0, None)), flush=True)
+        else:
+            print(json.dumps(adjoint_leg(args, fcu, wl, 1, 0)), flush=True)
+    elif args.grid_only:
         import torch
         torch.cuda.set_device(0)
         fcu = load("fluidcu", os.path.join(PKG, "fluidcu.py"))
