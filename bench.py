@@ -52,7 +52,11 @@ PKG = os.path.join(ROOT, "fluid-simulation-app_b200")
 WORKLOAD = "tilt_1m"
 METRIC = "particle-steps/s at 0.1% density error: plain vs batched vs adjoint, 1×B200"
 UNIT = "particle-steps/s"
+# The batched and adjoint legs run four substeps per 1/120 s frame
+# (substeps_for's floor at 5 mm spacing, render.rs:63-65); the plain step
+# runs the reference's whole policy, capped at SUBSTEP_CAP.
 SUBSTEPS_PER_FRAME = 4
+SUBSTEP_CAP = 16
 
 # Algorithmic bytes per particle of each substep kernel: the particle's own
 # records it must read and write once (neighbour reads are cache hits in
@@ -77,9 +81,9 @@ def workload_config(w, n):
     return {"workload": WORKLOAD, "particles": n, "lattice": "x".join(str(v) for v in w["lattice"]),
             "box_m": "x".join(str(v) for v in w["box_hi"]), "spacing_m": w["spacing"], "h_ratio": 1.2,
             "tracers": w["tracers"], "frame_dt_s": float(np.float32(1.0 / 120.0)),
-            "step": "one 1/120 s frame: 4 DFSPH substeps (substeps_for's floor at 5 mm), "
-                    "reduce_stats, one tracer pass; the metric counts substeps",
-            "substeps_per_frame": SUBSTEPS_PER_FRAME,
+            "step": "one 1/120 s frame: the policy's DFSPH substeps, reduce_stats, one tracer "
+                    "pass; the metric counts substeps",
+            "substeps_per_frame": "substeps_for on the one-frame-stale v_max (render.rs:3090-3094), cap 16",
             "solve": "tolerance div 1% / den 0.1%, cap 100, FP64 residuals",
             "tilt": "seed 1, three sinusoids per axis, <= 35 degrees, 0.2-2 Hz",
             "l2": "working set > 126 MB L2; no flush"}
@@ -203,15 +207,16 @@ def cuda_arm(args):
     forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
     dt = float(np.float32(1.0 / 120.0))
 
-    # Substeps per frame: substeps_for's floor at this spacing (render.rs:63-65,
-    # dt / (0.42 spacing) rounded up, four at 5 mm). Fixed rather than driven
-    # by the one-frame-stale v_max, so the device-timed and the end-to-end
-    # runs execute the same substeps on the same states.
-    sub = SUBSTEPS_PER_FRAME
-
+    # Substeps per frame: the reference's policy, substeps_for on the
+    # one-frame-stale v_max with a cap of 16 (render.rs:57-106, :3090-3094),
+    # which fluid_sim_frame applies when given no count. Each frame is
+    # followed by a sync, so the stale v_max is exactly the previous frame's
+    # in the device-timed loop as in the end-to-end loop and the reference
+    # arm, and all three execute the same substeps on the same states.
     def frame(sim, k):
         f = forces[k]
-        sim.frame((float(f[0]), float(f[1]), float(f[2])), dt, substeps=sub, cap=16, seed=k)
+        sim.frame((float(f[0]), float(f[1]), float(f[2])), dt, substeps=0, cap=SUBSTEP_CAP, seed=k)
+        sim.sync()
 
     cfg = wl.make_config(fcu, WORKLOAD, device=local)
     sim = fcu.Sim(cfg)
@@ -220,7 +225,7 @@ def cuda_arm(args):
         frame(sim, k)
     sim.sync()
     if args.profile_substeps:
-        return profile_only(args, fcu, wl, sim, forces, dt / sub, w)
+        return profile_only(args, fcu, wl, sim, forces, dt / SUBSTEPS_PER_FRAME, w)
     before = sim.stats()
     if world > 1:
         torch.distributed.barrier()
@@ -297,9 +302,10 @@ def cuda_arm(args):
 
     # roofline: per-kernel CUDA-event times of a few substeps of this state
     prof = {}
+    per_frame = max(1, int(round(substeps / args.steps)))
     for k in range(8):
         f = forces[(frames + k) % len(forces)]
-        dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
+        dts = float(np.float32(dt) / np.float32(per_frame))
         st = fcu.make_step(force=tuple(float(x) for x in f), dt=dts, v_clamp=wl.v_clamp(w["spacing"], dts))
         for name, t in sim.profile_step(st):
             prof.setdefault(name, []).append(t)
@@ -325,7 +331,7 @@ def cuda_arm(args):
     # the CPU oracle on this host over one substep of the same state
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample(fcu, sim, dt)
+        cpu = cpu_sample(fcu, sim, dt, per_frame)
 
     # the neighbour list the sweeps stream: 8 bytes per entry
     mean_nbrs = float(np.mean(sim.field("nbr_n").astype(np.float64)))
@@ -657,7 +663,7 @@ def finish_without_e2e(args, sim, value, ms_max, substeps, launches, clocks, wor
         torch.distributed.destroy_process_group()
 
 
-def cpu_sample(fcu, sim, dt):
+def cpu_sample(fcu, sim, dt, per_frame):
     """The oracle over one substep of the GPU's current state, all cores."""
     sys.path.insert(0, ROOT)
     from oracle import oracle as orc
@@ -672,7 +678,7 @@ def cpu_sample(fcu, sim, dt):
     o = orc.Sim(p, 0)
     st = sim.state()
     o.set_state(st["pos"], st["vel"], st["prev_vel"], st["prev_p"], st["temp"], st["id"])
-    dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
+    dts = float(np.float32(dt) / np.float32(per_frame))
     step = orc.make_step(force=(0.0, -9.81, 0.0), dt=dts,
                          v_clamp=float(np.float32(0.4) * np.float32(0.005) / np.float32(dts)))
     t0 = time.perf_counter()
@@ -710,17 +716,21 @@ def reference_arm(args):
     frames = args.warmup + args.steps
     forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
     dt = float(np.float32(1.0 / 120.0))
-    dts = float(np.float32(dt) / np.float32(SUBSTEPS_PER_FRAME))
-    vc = float(np.float32(0.4) * np.float32(spacing) / np.float32(dts))
-    iters = np.zeros(2, np.int64)
+    iters = np.zeros(3, np.int64)  # divergence, density iterations, substeps
+    v_max = [0.0]
 
     def frame(k):
+        # the reference's policy on the one-frame-stale v_max (render.rs:3090-3094)
         f = tuple(float(x) for x in forces[k])
+        m = orc.substeps_for(dt, v_max[0], spacing, SUBSTEP_CAP)
+        dts = float(np.float32(dt) / np.float32(m))
+        vc = float(np.float32(0.4) * np.float32(spacing) / np.float32(dts))
         st = orc.make_step(force=f, dt=dts, v_clamp=vc)
-        for _ in range(SUBSTEPS_PER_FRAME):
+        for _ in range(m):
             it, _ = o.substep_tol(st, 0.01, 0.001, 100)
-            iters[:] += it
-        o.stats()
+            iters[:2] += it
+        iters[2] += m
+        v_max[0] = float(o.stats()[6])
         o.tracer_pass(orc.make_step(force=f, dt=dt, seed=k))
 
     for k in range(args.warmup):
@@ -731,7 +741,7 @@ def reference_arm(args):
         frame(k)
     t = time.perf_counter() - t0
     final = o.stats()
-    substeps = SUBSTEPS_PER_FRAME * args.steps
+    substeps = int(iters[2])
     value = n * substeps / t
     cores = os.cpu_count()
     print(json.dumps({

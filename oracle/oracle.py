@@ -334,3 +334,36 @@ def field_filter(field2, ex, ey):
     lib().or_field_filter(f32(field2), w, h, ex, ey, out)
     return out
 
+
+
+# ---- the frame's substep policy (render.rs:57-106), restated ----------------
+# The reference picks each frame's substep count on the host from the
+# one-frame-stale v_max (render.rs:3090-3094). Float32 arithmetic as Rust's
+# f32, `as u32` saturating.
+_F = np.float32
+
+
+def _sat_u32(v):
+    v = float(v)
+    if not v > 0.0:
+        return 0
+    return 0xFFFFFFFF if v >= 4294967296.0 else int(v)
+
+
+def refine_passes(dt_sub):
+    return 5 if _F(dt_sub) > _F(0.00105) else 2
+
+
+def substep_floor(dt, dt_sub_max):
+    return min(_sat_u32(np.ceil(_F(dt) / _F(dt_sub_max))), 8)
+
+
+def substeps_for(dt, v_max, spacing, cap):
+    dt, v_max, spacing = _F(dt), _F(v_max), _F(spacing)
+    n = _sat_u32(np.ceil(dt * v_max / (_F(0.4) * spacing)))
+    n = max(n, substep_floor(dt, _F(0.42) * spacing))
+    cheap = _sat_u32(np.ceil(_F(1.0) / _F(120.0) / _F(0.00105)))
+    jump = refine_passes(dt / _F(cheap)) == 2 and n < cheap and _F(n) > _F(0.65) * _F(cheap)
+    if jump:
+        n = cheap
+    return min(n, cap)

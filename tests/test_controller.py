@@ -160,3 +160,16 @@ def test_the_first_frame_and_a_pause_encode_no_solve(fcu):
     p = ctl.plan([0, -1, 0], now_ms=100.0 + 1000.0 / 120.0 + 2000.0)
     assert abs(p.dt - 1.0 / 30.0) < 1e-7, "MAX_DT clamps a resume"
     assert abs(p.step.v_clamp - 0.4 * 0.01 / p.step.dt) < 1e-3
+
+
+# The oracle's restatement of the substep policy (the benchmark's reference
+# arm picks its substeps with it) agrees with the product's.
+def test_the_oracle_substep_policy_agrees_with_the_product(fcu, orc):
+    rng = np.random.default_rng(9)
+    dts = [float(F32(1.0) / F32(120.0)), float(F32(1.0) / F32(60.0)), 0.01, 0.004]
+    for dt in dts:
+        for spacing in (0.005, 0.0062, 0.01):
+            for v in np.concatenate([rng.uniform(0.0, 5.0, 200), [0.0, 1e6, np.inf]]):
+                v = float(F32(v))
+                assert orc.substeps_for(dt, v, spacing, 16) == fcu.substeps_for(dt, v, spacing, 16), \
+                    (dt, spacing, v)

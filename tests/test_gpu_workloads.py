@@ -96,6 +96,10 @@ WARMUP_FRAMES = 5
 CHECKED_FRAMES = 2
 
 
+# The benchmark's frames: substeps_for on the one-frame-stale v_max
+# (render.rs:3090-3094), a sync after every frame so the stale value is the
+# previous frame's. The oracle side picks its count with its own restatement
+# of the policy from its own statistics.
 def test_tilt_1m_frames_match_the_oracle(fcu, orc, wl):
     cfg = wl.make_config(fcu, "tilt_1m")
     sim = fcu.Sim(cfg)
@@ -104,18 +108,43 @@ def test_tilt_1m_frames_match_the_oracle(fcu, orc, wl):
     forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
     dt = float(F32(1.0 / 120.0))
     for k in range(WARMUP_FRAMES):
-        sim.frame(tuple(float(x) for x in forces[k]), dt, substeps=4, cap=16, seed=k)
-    sim.sync()
+        sim.frame(tuple(float(x) for x in forces[k]), dt, substeps=0, cap=16, seed=k)
+        sim.sync()
     o = oracle_of(orc, sim)
-    iters = []
+    v_max = sim.stats().v_max
+    counts = []
     for k in range(WARMUP_FRAMES, frames):
         force = tuple(float(x) for x in forces[k])
         before = Before(sim, o)
-        sim.frame(force, dt, substeps=4, cap=16, seed=k)
-        its, ostats = oracle_frame(orc, o, cfg, force, dt, 4, k, True)
-        iters.append(compare_frame(sim, o, its, ostats, before, f"tilt_1m frame {k}"))
-    # the solve really iterated, as in the benchmark's window
-    assert all(d >= 4 and e >= 8 for d, e in iters), iters
+        m = orc.substeps_for(dt, v_max, cfg.spacing, 16)
+        sim.frame(force, dt, substeps=0, cap=16, seed=k)
+        sim.sync()
+        assert sim.stats().substeps_last_frame == m, (k, m)
+        its, ostats = oracle_frame(orc, o, cfg, force, dt, m, k, True)
+        compare_frame(sim, o, its, ostats, before, f"tilt_1m frame {k}")
+        v_max = float(ostats[6])
+        counts.append(m)
+    # the tilt moves the fluid past the 4-substep floor's CFL speed
+    assert max(counts) > 4, counts
+    sim.close()
+
+
+def test_tilt_1m_fixed_four_substep_frames_match_the_oracle(fcu, orc, wl):
+    cfg = wl.make_config(fcu, "tilt_1m")
+    sim = fcu.Sim(cfg)
+    frames = WARMUP_FRAMES + 1
+    forces = wl.tilt_schedule(1, frames, 1.0 / 120.0)
+    dt = float(F32(1.0 / 120.0))
+    for k in range(WARMUP_FRAMES):
+        sim.frame(tuple(float(x) for x in forces[k]), dt, substeps=4, cap=16, seed=k)
+    sim.sync()
+    o = oracle_of(orc, sim)
+    force = tuple(float(x) for x in forces[WARMUP_FRAMES])
+    before = Before(sim, o)
+    sim.frame(force, dt, substeps=4, cap=16, seed=WARMUP_FRAMES)
+    its, ostats = oracle_frame(orc, o, cfg, force, dt, 4, WARMUP_FRAMES, True)
+    d, e = compare_frame(sim, o, its, ostats, before, "tilt_1m fixed four")
+    assert d >= 4 and e >= 8, (d, e)  # the solve really iterated
     sim.close()
 
 
