@@ -4,10 +4,12 @@ tilt_1m is built exactly as the benchmark builds it (box geometry, h = 1.2
 spacing, tolerance solve with FP64 residuals, a seeded tilt per frame, 4,096
 tracers, 1,048,576 particles) and advanced through fluid_sim_frame, the call
 the benchmark times: after the benchmark's warm-up frames the GPU state and
-tracers are copied into the oracle, and both take the next frames: four
-substeps of the tolerance solve, reduce_stats and a tracer pass each. The
-particle state, the tracers, the statistics block, the iteration counts and
-the FP64 residuals must be identical.
+tracers are copied into the oracle, and both take the next frames: the
+substeps the reference's policy picks from the one-frame-stale v_max, each
+a tolerance solve, then reduce_stats and a tracer pass. The substep counts,
+the particle state, the tracers, the statistics block, the iteration counts
+and the FP64 residuals must be identical. A frame at a fixed four substeps
+is compared the same way.
 
 dam_break_16k (16,384 particles, two substeps per 1/120 s frame, tolerance
 solve) is run for ten frames from its initial lattice the same way and
