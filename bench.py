@@ -438,7 +438,8 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     final = batch.stats()
     sub = len(steps) - nw
     local_rows = [[a.total_den_iters - b.total_den_iters, a.total_div_iters - b.total_div_iters,
-                   f.compression_avg, f.compression_max] for a, b, f in zip(after, before, final)]
+                   f.compression_avg, f.compression_max, a.clamp_count - b.clamp_count]
+                  for a, b, f in zip(after, before, final)]
     rows = sharding.gather_box_values(mine, local_rows, len(cfgs_all),
                                       device="cuda" if world > 1 else "cpu")
     if world > 1:
@@ -459,6 +460,7 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
             "mean_div_iters_per_box": float(rows[:, 1].mean() / sub),
             "compression_avg_mean": float(rows[:, 2].mean()),
             "compression_avg_worst_box": float(rows[:, 2].max()),
+            "clamps_per_particle_substep": float(rows[:, 4].sum() / (total * sub)),
             "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu if plain_per_gpu else None,
             "vs_the_same_boxes_as_plain_sims": plain_boxes,
             "autotuned_blocks": chosen,
