@@ -130,3 +130,59 @@ def test_the_forward_is_deterministic_and_checkpoints_do_not_change_it(fcu, wl):
     assert a.forward(forces, 0.01, target) == la
     ga2, xa2 = a.backward()
     assert np.array_equal(ga2.view(np.uint64), ga.view(np.uint64)) and xa2 == xa
+
+
+# The adjoint workload's own box: the 64x16x64 block (65,536 particles) of
+# the benchmark's adjoint leg, checkpoints every 10 frames, 16 seeded
+# directions, FP64 central differences. Four frames (16 substeps) is the
+# longest horizon at which central differences at two step sizes agree:
+# measured on this box, at 4 frames steps 1e-6 and 5e-7 agree with each other
+# and with the adjoint to 1e-7, while at 6 frames the differences at steps
+# 1e-4 .. 1e-6 differ from one another by 10-60 % (the loss is only piecewise
+# smooth there: pairs cross the support radius and clamps switch within the
+# step, and the sensitivity grows five- to tenfold a frame, |g| 8e-4 at 2
+# frames, 6e-3 at 6, 1e2 at 10).
+CONFIG4_FRAMES = 4
+
+
+def test_fp64_adjoint_on_the_adjoint_workloads_box(fcu, wl):
+    frames = CONFIG4_FRAMES
+    cfg = wl.make_config(fcu, "adjoint_64k")
+    dt = float(np.float32(1.0 / 120.0))
+    dts = float(np.float32(dt) / np.float32(SPF))
+    vc = wl.v_clamp(0.005, dts)
+    forces = wl.tilt_schedule(2, frames, 1.0 / 120.0).astype(np.float64)
+    target = np.array([0.64, 0.05, 0.64])
+    a32 = fcu.Adjoint(cfg, frames, SPF, dt, vc, 10, precision=32)
+    assert a32.n == 65536
+    a32.forward(forces, 0.01, target)
+    sched = a32.schedule()
+    a64 = fcu.Adjoint(cfg, frames, SPF, dt, vc, 10, precision=64)
+    a64.set_schedule(*sched)
+    a64.forward(forces, 0.01, target)
+    g, gx = a64.backward()
+    gv = np.concatenate([g.ravel(), [gx]])
+    # one checkpoint per frame recomputes four segments: the same bits
+    a1 = fcu.Adjoint(cfg, frames, SPF, dt, vc, 1, precision=64)
+    a1.set_schedule(*sched)
+    a1.forward(forces, 0.01, target)
+    g1, gx1 = a1.backward()
+    assert np.array_equal(g1.view(np.uint64), g.view(np.uint64)) and gx1 == gx
+    u0 = np.concatenate([forces.ravel(), [0.01]])
+    rng = np.random.default_rng(16)
+    floor = 1e-3 * np.linalg.norm(gv)
+    worst = 0.0
+    for k in range(16):
+        d = rng.normal(size=u0.size)
+        d /= np.linalg.norm(d)
+        fd = {}
+        for h in (1e-6, 5e-7):
+            lp = a64.forward((u0 + h * d)[:-1], (u0 + h * d)[-1], target)
+            lm = a64.forward((u0 - h * d)[:-1], (u0 - h * d)[-1], target)
+            fd[h] = (lp - lm) / (2 * h)
+        scale = max(abs(fd[1e-6]), floor)
+        assert abs(fd[1e-6] - fd[5e-7]) <= 1e-3 * scale, (k, fd)  # the two steps agree
+        rel = abs(float(gv @ d) - fd[1e-6]) / scale
+        worst = max(worst, rel)
+        assert rel <= 1e-3, (k, float(gv @ d), fd)
+    print(f"adjoint_64k box, {frames} frames: worst relative error over 16 directions {worst:.3g}")
