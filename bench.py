@@ -300,6 +300,11 @@ def cuda_arm(args):
     e2e_value = n * e2e_all / e2e_s
     sim_e.close()
 
+    # The same frames at a fixed four substeps (substeps_for's floor at 5 mm,
+    # render.rs:63-65) on a fresh replica, device-timed without syncs: the
+    # CFL clamp then catches the fast particles instead of more substeps.
+    fixed = fixed_four_leg(args, fcu, wl, forces, dt, local) if not args.no_fixed else None
+
     # roofline: per-kernel CUDA-event times of a few substeps of this state
     prof = {}
     per_frame = max(1, int(round(substeps / args.steps)))
@@ -368,6 +373,7 @@ def cuda_arm(args):
             "cpu_baseline": cpu,
             "clocks": clocks.summary(),
             "gpu_launches": launches,
+            "fixed_four_substeps": fixed,
             "batched": batched,
             "adjoint": adjoint,
             "grid": grid,
@@ -395,10 +401,13 @@ BATCH_FRAMES = 30
 def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     """The batched workload: 256 boxes of 4,096..65,536 particles (log-
     uniform, about 5.7M in all), each with its own tilt sequence and XSPH
-    coefficient, 4 substeps per 1/120 s frame, tolerance solve. Each rank
-    steps its LPT shard of the boxes as one batch (no collective in the
-    step); device time on the batch's stream, max over ranks; per-box
-    statistics are summed across ranks at the end."""
+    coefficient, tolerance solve. The boxes share one substep clock: each
+    1/120 s frame runs the most substeps the reference's policy asks for
+    any box (substeps_for on that box's one-frame-stale v_max, cap 16), all
+    boxes at that frame's dt. Each rank steps its LPT shard of the boxes as
+    one batch (no collective in the step); device time on the batch's
+    stream, max over ranks; per-box statistics are summed across ranks at
+    the end."""
     import torch
     sharding = load("sharding", os.path.join(PKG, "sharding.py"))
     cfgs_all = wl.batched_boxes(fcu, nboxes=args.boxes)
@@ -408,15 +417,34 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     for c in cfgs:
         c.device = local
     batch = fcu.Batch(cfgs)
-    steps_all = wl.batched_frame_steps(fcu, len(cfgs_all), BATCH_WARMUP_FRAMES + BATCH_FRAMES,
-                                       substeps=SUBSTEPS_PER_FRAME)
-    steps = [[row[b] for b in mine] for row in steps_all]
-    nw = BATCH_WARMUP_FRAMES * SUBSTEPS_PER_FRAME
-    batch.run(steps[:nw])
-    batch.sync()
+    frames = BATCH_WARMUP_FRAMES + BATCH_FRAMES
+    dt = float(np.float32(1.0 / 120.0))
+    forces = [wl.tilt_schedule(3 * 100003 + b, frames, 1.0 / 120.0) for b in mine]
+    v_max = [0.0] * len(mine)
+    recorded = []
+
+    def frame_steps(k):
+        n = max(fcu.substeps_for(dt, v, wl.BATCH_SPACING, SUBSTEP_CAP) for v in v_max)
+        dts = float(np.float32(dt) / np.float32(n))
+        vc = wl.v_clamp(wl.BATCH_SPACING, dts)
+        row = [fcu.make_step(force=tuple(float(x) for x in forces[q][k]), dt=dts, v_clamp=vc, seed=k)
+               for q in range(len(mine))]
+        return [row] * n
+
+    def frame(k):
+        steps = frame_steps(k)
+        batch.run(steps)
+        batch.reduce_stats()
+        v_max[:] = [st.v_max for st in batch.stats()]  # synchronises: the next frame's stale v_max
+        recorded.extend(steps)
+        return len(steps)
+
+    for k in range(BATCH_WARMUP_FRAMES):
+        frame(k)
+    nw = len(recorded)
     # block sizes from the autotuner (one timed substep per candidate on the
     # warmed-up state, which it restores)
-    chosen, tune_ms = batch.autotune(steps[nw])
+    chosen, tune_ms = batch.autotune(frame_steps(BATCH_WARMUP_FRAMES)[0])
     before = batch.stats()
     stream = torch.cuda.ExternalStream(batch.stream())
     if world > 1:
@@ -424,43 +452,44 @@ def batched_leg(args, fcu, wl, world, rank, local, plain_per_gpu):
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e2 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    batch.run(steps[nw:nw + PLAIN_BOX_SUBSTEPS])
+    sub = sum(frame(k) for k in range(BATCH_WARMUP_FRAMES, frames))
     e1.record(stream)
-    batch.run(steps[nw + PLAIN_BOX_SUBSTEPS:])
-    e2.record(stream)
-    e2.synchronize()
-    ms = e0.elapsed_time(e2)
-    ms_head = e0.elapsed_time(e1)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
     after = batch.stats()
-    batch.reduce_stats()
-    final = batch.stats()
-    sub = len(steps) - nw
     local_rows = [[a.total_den_iters - b.total_den_iters, a.total_div_iters - b.total_div_iters,
-                   f.compression_avg, f.compression_max, a.clamp_count - b.clamp_count]
-                  for a, b, f in zip(after, before, final)]
+                   a.compression_avg, a.compression_max, a.clamp_count - b.clamp_count]
+                  for a, b in zip(after, before)]
     rows = sharding.gather_box_values(mine, local_rows, len(cfgs_all),
                                       device="cuda" if world > 1 else "cpu")
+    work = float(sum(counts[b] for b in mine) * sub)  # particle-substeps of this rank
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t[0])
+        wt = torch.tensor([work], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(wt, op=torch.distributed.ReduceOp.SUM)
+        work = float(wt[0])
     total = int(sum(counts))
-    value = total * sub / (ms / 1000.0)
+    value = work / (ms / 1000.0)
     batch.close()
     plain_boxes = None
     if world == 1 and not args.no_plain_boxes:
-        plain_boxes = plain_boxes_leg(fcu, cfgs, steps, nw, total * PLAIN_BOX_SUBSTEPS / (ms_head / 1000.0))
+        plain_boxes = plain_boxes_leg(fcu, cfgs, recorded, nw, value)
+    per_box_substeps = work / total
     return {"workload": "batched_256", "boxes": len(cfgs_all), "particles": total,
-            "substeps": sub, "warmup_substeps": nw, "ms_per_substep": ms / sub, "value": value,
-            "unit": UNIT, "sharding": f"LPT over {world} rank(s)" if world > 1 else "one batch",
+            "frames": BATCH_FRAMES, "substeps": sub, "substeps_per_frame": sub / BATCH_FRAMES,
+            "warmup_substeps": nw, "ms_per_substep": ms / sub, "ms_per_frame": ms / BATCH_FRAMES,
+            "value": value, "unit": UNIT,
+            "step": "substeps_for on each box's one-frame-stale v_max, the most any box asks for, cap 16",
+            "sharding": f"LPT over {world} rank(s)" if world > 1 else "one batch",
             "scaling": "strong",
-            "mean_den_iters_per_box": float(rows[:, 0].mean() / sub),
-            "mean_div_iters_per_box": float(rows[:, 1].mean() / sub),
+            "mean_den_iters_per_box": float(rows[:, 0].mean() / per_box_substeps),
+            "mean_div_iters_per_box": float(rows[:, 1].mean() / per_box_substeps),
             "compression_avg_mean": float(rows[:, 2].mean()),
             "compression_avg_worst_box": float(rows[:, 2].max()),
-            "clamps_per_particle_substep": float(rows[:, 4].sum() / (total * sub)),
+            "clamps_per_particle_substep": float(rows[:, 4].sum() / work),
             "vs_plain_tilt_1m_per_gpu": value / world / plain_per_gpu if plain_per_gpu else None,
             "vs_the_same_boxes_as_plain_sims": plain_boxes,
             "autotuned_blocks": chosen,
@@ -478,7 +507,8 @@ def plain_boxes_leg(fcu, cfgs, steps, nw, batch_value):
     another, each box's substeps then a device sync, and (b) every box's
     substeps enqueued on its own stream, then one sync. Wall clock around
     device syncs (the work spans 256 streams). Same Step blocks and the same
-    per-box results (each box bit-identical to the batch's)."""
+    per-box results (each box bit-identical to the batch's); compared with
+    the batch's rate over its timed frames."""
     import torch
     sims = [fcu.Sim(c) for c in cfgs]
     try:
@@ -501,7 +531,7 @@ def plain_boxes_leg(fcu, cfgs, steps, nw, batch_value):
             s.close()
     work = sum(counts) * len(timed)
     one_by_one, concurrent = work / (t1 - t0), work / (t2 - t1)
-    return {"substeps": len(timed), "batch_on_these_substeps": batch_value,
+    return {"substeps": len(timed), "batch": batch_value,
             "one_box_at_a_time": one_by_one, "all_boxes_on_own_streams": concurrent,
             "batch_over_one_at_a_time": batch_value / one_by_one,
             "batch_over_concurrent": batch_value / concurrent}
@@ -665,6 +695,38 @@ def finish_without_e2e(args, sim, value, ms_max, substeps, launches, clocks, wor
         torch.distributed.destroy_process_group()
 
 
+def fixed_four_leg(args, fcu, wl, forces, dt, local):
+    import torch
+    sim = fcu.Sim(wl.make_config(fcu, WORKLOAD, device=local))
+
+    def frame(k):
+        f = forces[k]
+        sim.frame((float(f[0]), float(f[1]), float(f[2])), dt, substeps=SUBSTEPS_PER_FRAME, cap=16, seed=k)
+
+    for k in range(args.warmup):
+        frame(k)
+    sim.sync()
+    b = sim.stats()
+    stream = torch.cuda.ExternalStream(sim.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(args.warmup, args.warmup + args.steps):
+        frame(k)
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    a = sim.stats()
+    sub = int(a.substeps - b.substeps)
+    out = {"substeps_per_frame": SUBSTEPS_PER_FRAME, "value": sim.n * sub / (ms / 1000.0), "unit": UNIT,
+           "ms_per_frame": ms / args.steps,
+           "mean_den_iters": (a.total_den_iters - b.total_den_iters) / max(sub, 1),
+           "clamps_per_particle_substep": (a.clamp_count - b.clamp_count) / float(sim.n * max(sub, 1)),
+           "compression_avg": a.compression_avg}
+    sim.close()
+    return out
+
+
 def cpu_sample(fcu, sim, dt, per_frame):
     """The oracle over one substep of the GPU's current state, all cores."""
     sys.path.insert(0, ROOT)
@@ -774,6 +836,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-boxes leg")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint leg")
     ap.add_argument("--no-grid", action="store_true", help="skip the 16.7M-position grid leg")
+    ap.add_argument("--no-fixed", action="store_true", help="skip the fixed-four-substep frames")
     ap.add_argument("--no-plain-boxes", action="store_true",
                     help="skip stepping the batched boxes as separate plain sims")
     ap.add_argument("--profile-substeps", type=int, default=0,

@@ -356,11 +356,6 @@ static_assert(kRadix == kSortThreads, "one thread per digit");
 #ifndef FCU_SORT_MATCH
 #define FCU_SORT_MATCH 0
 #endif
-// FCU_SORT_PACK: a tile's keys and values staged together as 8-byte words
-// (one shared store and one load per element instead of two).
-#ifndef FCU_SORT_PACK
-#define FCU_SORT_PACK 0
-#endif
 
 __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
     const uint32_t *__restrict__ keys_in, const uint32_t *__restrict__ vals_in, uint32_t n, int shift,
@@ -372,12 +367,8 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
     __shared__ uint32_t s_start[kRadix];  // staged index of the tile's first element of digit d
     __shared__ uint32_t s_wsum[kSortWarps];
     __shared__ uint32_t s_gsum[kSortWarps];
-#if FCU_SORT_PACK
-    __shared__ uint2 s_kv[kSortTile];  // (key, value) staged as one 8-byte word
-#else
     __shared__ uint32_t s_key[kSortTile];
     __shared__ uint32_t s_val[kSortTile];
-#endif
     __shared__ uint32_t s_tile;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
@@ -487,41 +478,24 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
         if (i < n) {
             const uint32_t d = (key[r] >> shift) & (kRadix - 1);
             const uint32_t at = s_start[d] + s_hist[warp][d] + rank[r];
-#if FCU_SORT_PACK
-            s_kv[at] = make_uint2(key[r], vals_in ? __ldg(&vals_in[i]) : (uint32_t)i);
-#else
             s_key[at] = key[r];
             s_val[at] = vals_in ? __ldg(&vals_in[i]) : (uint32_t)i;
-#endif
         }
     }
     __syncthreads();
     const uint64_t tbase = (uint64_t)tile * kSortTile;
     const uint32_t count = (uint32_t)(n - tbase < kSortTile ? n - tbase : kSortTile);
     for (uint32_t j = threadIdx.x; j < count; j += kSortThreads) {
-#if FCU_SORT_PACK
-        const uint2 kv = s_kv[j];
-        const uint32_t k = kv.x;
-#else
         const uint32_t k = s_key[j];
-#endif
         const uint32_t d = (k >> shift) & (kRadix - 1);
         const uint32_t dst = s_off[d] + (j - s_start[d]);
         // Always below n when the counts are right; the test keeps a
         // look-back that gave up (garbage offsets) from writing out of bounds.
         if (dst < n) {
-#if FCU_SORT_PACK
-            vals_out[dst] = kv.y;
-#else
             vals_out[dst] = s_val[j];
-#endif
             if (keys_out) keys_out[dst] = k;
             if (starts && k < cells) {
-#if FCU_SORT_PACK
-                const uint32_t kn = j + 1 < count ? s_kv[j + 1].x : 0u;
-#else
                 const uint32_t kn = j + 1 < count ? s_key[j + 1] : 0u;
-#endif
                 const bool seg_end = j + 1 == count || ((kn >> shift) & (kRadix - 1)) != d;
                 if (seg_end) atomicMax(&starts[k + 1], dst + 1);
                 else if (kn != k) starts[k + 1] = dst + 1;

@@ -54,11 +54,6 @@ constexpr int kBatchKappaThreads = 768;
 #ifndef FCU_DD_CHUNK
 #define FCU_DD_CHUNK 4
 #endif
-// FCU_TILED_KAPPA > 0: the one-box den_kappa runs list-free, cell-tiled
-// (k_den_kappa_tiled) with that many cells per tile.
-#ifndef FCU_TILED_KAPPA
-#define FCU_TILED_KAPPA 0
-#endif
 #ifndef FCU_MINB
 #define FCU_MINB 0
 #endif
@@ -318,7 +313,6 @@ __device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, 
 #endif
 }
 
-#if FCU_GRAD_LIST
 // The same walk over the gradient list: each entry carries the pair's
 // kernel gradient itself (slot in w), `use(gradient, record)`.
 __device__ __forceinline__ float4 glist_ld(const float4 *p) {
@@ -358,7 +352,6 @@ __device__ __forceinline__ void walk_grad(const float4 *__restrict__ nbr, uint32
         for (int u = 0; u < B; ++u) e[u] = en[u];
     }
 }
-#endif
 
 struct PosKd {
     float4 p;
@@ -536,9 +529,7 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
                 const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]), gw);
                 if (found < P.nbr_cap) {
                     b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
-#if FCU_GRAD_LIST
-                    b.nbr_g[(size_t)found * n + i] = make_float4(gw.x, gw.y, gw.z, __uint_as_float(k));
-#endif
+                    if (b.nbr_g) b.nbr_g[(size_t)found * n + i] = make_float4(gw.x, gw.y, gw.z, __uint_as_float(k));
                 }
                 found++;
             }
@@ -661,10 +652,9 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
                             const uint32_t idx = found + h + u;
                             if (idx < cap) {
                                 b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
-#if FCU_GRAD_LIST
-                                b.nbr_g[(size_t)idx * n + i] =
-                                    make_float4(gw.x, gw.y, gw.z, __uint_as_float(j[u]));
-#endif
+                                if (!kB)
+                                    b.nbr_g[(size_t)idx * n + i] =
+                                        make_float4(gw.x, gw.y, gw.z, __uint_as_float(j[u]));
                             }
                         }
                     }
@@ -954,16 +944,17 @@ __device__ __forceinline__ void den_kappa_at(const Geo &g, const SimBufs &b, uin
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
         float drho = 0.0f;
-#if FCU_GRAD_LIST
-        walk_grad<FCU_B_PV, float4>(
-            b.nbr_g, n, i, cnt, [&](uint32_t j) { return __ldg(&b.wvel[j]); },
-            [&](F3 gw, const float4 &v) { drho += dot(vel - xyz(v), gw); });
-#else
-        walk<FCU_B_PV, PosVel>(
-            b.nbr, n, i, cnt,
-            [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
-            [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
-#endif
+        if (!kB) {
+            // one box: the gradient list, one velocity record per neighbour
+            walk_grad<FCU_B_PV, float4>(
+                b.nbr_g, n, i, cnt, [&](uint32_t j) { return __ldg(&b.wvel[j]); },
+                [&](F3 gw, const float4 &v) { drho += dot(vel - xyz(v), gw); });
+        } else {
+            walk<FCU_B_PV, PosVel>(
+                b.nbr, n, i, cnt,
+                [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
+                [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
+        }
         const float rho = __ldg(&b.density[i]);
         drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;
@@ -1043,126 +1034,6 @@ __global__ void __launch_bounds__(kListTile, FCU_MINB) k_forces_div_list(Geo g, 
     }
 }
 
-// ---- den_kappa without the list, cell-tiled ----------------------------------
-// The same prediction as k_den_kappa with no neighbour list: each CTA takes
-// grid rows (y, z) in turn and walks a row in tiles of T x-adjacent cells.
-// A tile's particles draw their neighbours from nine slot ranges, one per
-// stencil row (oz, oy), each covering cells x0 - 1 .. x0 + T; those ranges'
-// positions and velocities are staged in shared memory with 128-bit loads,
-// once per tile. Each thread then tests its particle's 27-cell candidates in
-// stencil order (rows by oz then oy, slots ascending: the order density_div
-// found them in), r^2 < support^2 and not itself, stops after the list cap,
-// and sums the same pair terms with the gradient scale recomputed exactly as
-// density_div formed it (IEEE square root and division), so the sum is the
-// list walk's sum bit for bit. A tile whose neighbourhood does not fit the
-// staging area takes the list walk.
-template <int TPB, int T, int CAP>
-__global__ void __launch_bounds__(TPB) k_den_kappa_tiled(Geo g, SimBufs b, int slot) {
-    __shared__ float4 s_pos[CAP];
-    __shared__ float4 s_vel[CAP];
-    __shared__ uint32_t s_st[9][T + 3];  // starts of cells x0-1 .. x0+T+1 per stencil row (clamped)
-    __shared__ uint32_t s_off[9];        // shared index of each row's first staged slot
-    __shared__ uint32_t s_lo[9];         // global slot of each row's first staged slot
-    __shared__ uint32_t s_total;
-    const DevParams &P = g.one;
-    const uint32_t n = g.n, dx = P.dims[0], dy = P.dims[1], dz = P.dims[2];
-    const uint32_t rows = dy * dz, cap = P.nbr_cap;
-    const float mass = P.mass, rho0 = P.rho0, dt = g.st[0].s.dt;
-    unsigned long long term = 0;
-    for (uint32_t row = blockIdx.x; row < rows; row += gridDim.x) {
-        const uint32_t y = row % dy, z = row / dy;
-        const uint32_t rbase = row * dx;
-        if (__ldg(&b.starts[rbase]) == __ldg(&b.starts[rbase + dx])) continue;  // uniform: empty row
-        for (uint32_t x0 = 0; x0 < dx; x0 += T) {
-            const uint32_t x1 = x0 + T < dx ? x0 + T : dx;  // tile cells x0 .. x1 - 1
-            const uint32_t p0 = __ldg(&b.starts[rbase + x0]), p1 = __ldg(&b.starts[rbase + x1]);
-            if (p0 == p1) continue;
-            __syncthreads();  // the previous tile's staging is no longer read
-            if (threadIdx.x < 9u * (T + 3)) {
-                const uint32_t r = threadIdx.x / (T + 3), k = threadIdx.x % (T + 3);
-                const int cz = (int)z + (int)(r / 3) - 1, cy = (int)y + (int)(r % 3) - 1;
-                const int cx = (int)x0 - 1 + (int)k;
-                uint32_t v = 0;
-                if (cz >= 0 && cz < (int)dz && cy >= 0 && cy < (int)dy) {
-                    const uint32_t rb = ((uint32_t)cz * dy + (uint32_t)cy) * dx;
-                    const int c = cx < 0 ? 0 : (cx > (int)dx ? (int)dx : cx);
-                    v = __ldg(&b.starts[rb + (uint32_t)c]);
-                }
-                s_st[r][k] = v;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                uint32_t tot = 0;
-                for (int r = 0; r < 9; ++r) {
-                    // staged: cells max(x0-1, 0) .. min(x1, dx-1)
-                    const uint32_t a = s_st[r][x0 == 0 ? 1 : 0];
-                    const uint32_t e = s_st[r][(x1 < dx ? x1 : dx - 1) - x0 + 2];
-                    s_lo[r] = a;
-                    s_off[r] = tot;
-                    tot += e - a;
-                }
-                s_total = tot;
-            }
-            __syncthreads();
-            const uint32_t total = s_total;
-            const bool staged = total <= (uint32_t)CAP;
-            if (staged) {
-                for (int r = 0; r < 9; ++r) {
-                    const uint32_t a = s_lo[r], o = s_off[r];
-                    const uint32_t m = (r < 8 ? s_off[r + 1] : total) - o;
-                    for (uint32_t k = threadIdx.x; k < m; k += TPB) {
-                        s_pos[o + k] = __ldg(&b.wpos[a + k]);
-                        s_vel[o + k] = __ldg(&b.wvel[a + k]);
-                    }
-                }
-            }
-            __syncthreads();
-            for (uint32_t i = p0 + threadIdx.x; i < p1; i += TPB) {
-                const F3 pos = xyz(__ldg(&b.wpos[i]));
-                const F3 vel = xyz(__ldg(&b.wvel[i]));
-                float drho = 0.0f;
-                if (staged) {
-                    const uint32_t bx = axis_cell(pos.x, P.box_min[0], P.cell, dx);
-                    const uint32_t kx0 = bx > 0 ? bx - x0 : 1u;                      // cell max(bx-1, 0)
-                    const uint32_t kx1 = (bx + 1 < dx ? bx + 1 : dx - 1) - x0 + 2;  // cell min(bx+1, dx-1) + 1
-                    uint32_t found = 0;
-                    for (int r = 0; r < 9 && found < cap; ++r) {
-                        const uint32_t a = s_st[r][kx0], e = s_st[r][kx1];
-                        const int32_t sh = (int32_t)s_off[r] - (int32_t)s_lo[r];
-                        for (uint32_t j = a; j < e; ++j) {
-                            if (j == i) continue;
-                            const float4 pj = s_pos[(uint32_t)((int32_t)j + sh)];
-                            const F3 x = pos - xyz(pj);
-                            const float r2 = dot(x, x);
-                            if (r2 >= P.support_sq) continue;
-                            const float rr = sqrtf(r2);
-                            const float gs = grad_scale(P, rr, rr * P.inv_h);
-                            const float4 vj = s_vel[(uint32_t)((int32_t)j + sh)];
-                            drho += dot(vel - xyz(vj), gs * x);
-                            if (++found >= cap) break;
-                        }
-                    }
-                } else {
-                    walk<FCU_B_PV, PosVel>(
-                        b.nbr, n, i, __ldg(&b.nbr_n[i]),
-                        [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
-                        [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
-                }
-                const float rho = __ldg(&b.density[i]);
-                drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
-                const float rho_star = rho + dt * drho;
-                const float kk = fmaxf(rho_star - rho0, 0.0f) * __ldg(&b.alpha[i]) / (dt * dt);
-                const float kdv = kk / rho;
-                b.kd[i] = kdv;
-                b.wpk[i] = make_float4(pos.x, pos.y, pos.z, kdv);
-                b.pinc[i] = kk * rho;
-                term += fixed_term((double)rho_star / (double)rho0 - 1.0);
-            }
-        }
-    }
-    // one integer add per thread that summed anything: order-free
-    if (term) atomicAdd(&g.solve[0].acc_den[slot], term);
-}
 
 // ---- integrate (sim_solve.wgsl:709-756) ------------------------------------
 // With div_slot >= 0 (the fixed schedule) each box's first slot also records
@@ -1621,33 +1492,31 @@ void launch_forces_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot,
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b) {
     FCU_SWEEP(k_forces_apply, kTuneForcesApply, kSolveThreads, g, b);
 }
-void launch_den_kappa_tiled(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int cells_per_tile) {
-    if (!g.n || g.box_of) return;
-    const uint32_t rows = g.one.dims[1] * g.one.dims[2];
-    const uint32_t grid = rows < 148u * 8u ? rows : 148u * 8u;
-    if (cells_per_tile <= 2) k_den_kappa_tiled<128, 2, 512><<<grid, 128, 0, s>>>(g, b, slot);
-    else if (cells_per_tile <= 4) k_den_kappa_tiled<128, 4, 768><<<grid, 128, 0, s>>>(g, b, slot);
-    else k_den_kappa_tiled<128, 8, 1280><<<grid, 128, 0, s>>>(g, b, slot);
+// The persistent loop sweeps over a batch's work list: one wave of resident
+// kListTile-thread blocks (the list's length is only known on the device),
+// each striding over the tiles, so no block waits for a second wave.
+template <class K>
+uint32_t resident_blocks(K kernel) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, (int)kListTile, 0);
+    const uint32_t n = (uint32_t)(sms > 0 ? sms : 1) * (uint32_t)(per > 0 ? per : 1);
+    return n;
 }
-// The persistent loop sweeps over a batch's work list: a fixed grid (the
-// list's length is only known on the device) of kListTile-thread blocks.
-constexpr uint32_t kListBlocks = 148u * 6u;
 void launch_apply_list(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int which) {
-    k_apply_list<<<kListBlocks, kListTile, 0, s>>>(g, b, add_pressure ? 1 : 0, which);
+    static const uint32_t blocks = resident_blocks(k_apply_list);
+    k_apply_list<<<blocks, kListTile, 0, s>>>(g, b, add_pressure ? 1 : 0, which);
 }
 void launch_den_kappa_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which) {
-    k_den_kappa_list<<<kListBlocks, kListTile, 0, s>>>(g, b, slot, which);
+    static const uint32_t blocks = resident_blocks(k_den_kappa_list);
+    k_den_kappa_list<<<blocks, kListTile, 0, s>>>(g, b, slot, which);
 }
 void launch_forces_div_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which) {
-    k_forces_div_list<<<kListBlocks, kListTile, 0, s>>>(g, b, slot, which);
+    static const uint32_t blocks = resident_blocks(k_forces_div_list);
+    k_forces_div_list<<<blocks, kListTile, 0, s>>>(g, b, slot, which);
 }
 void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
-#if FCU_TILED_KAPPA
-    if (!g.box_of) {
-        launch_den_kappa_tiled(s, g, b, slot, FCU_TILED_KAPPA);
-        return;
-    }
-#endif
     FCU_SWEEP(k_den_kappa, kTuneDenKappa, kSolveThreads, g, b, slot, gate);
 }
 void launch_integrate(cudaStream_t s, const Geo &g, const SimBufs &b, int div_slot, int den_slot,
