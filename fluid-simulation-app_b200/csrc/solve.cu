@@ -313,46 +313,6 @@ __device__ __forceinline__ void walk(const uint2 *__restrict__ nbr, uint32_t n, 
 #endif
 }
 
-// The same walk over the gradient list: each entry carries the pair's
-// kernel gradient itself (slot in w), `use(gradient, record)`.
-__device__ __forceinline__ float4 glist_ld(const float4 *p) {
-#if FCU_LIST_CS
-    return __ldcs(p);
-#else
-    return __ldg(p);
-#endif
-}
-template <int B, class T, class Load, class Use>
-__device__ __forceinline__ void walk_grad(const float4 *__restrict__ nbr, uint32_t n, uint32_t i,
-                                          uint32_t cnt, Load load, Use use) {
-    float4 e[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u)
-        e[u] = ((uint32_t)u < cnt) ? glist_ld(&nbr[(size_t)u * n + i]) : make_float4(0.f, 0.f, 0.f, __uint_as_float(i));
-    for (uint32_t k = 0; k < cnt; k += B) {
-        T v[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u) v[u] = load(__float_as_uint(e[u].w));
-        float4 en[B];
-#pragma unroll
-        for (int u = 0; u < B; ++u)
-            en[u] = (k + B + u < cnt) ? glist_ld(&nbr[(size_t)(k + B + u) * n + i])
-                                      : make_float4(0.f, 0.f, 0.f, __uint_as_float(i));
-#if FCU_L2PF
-#pragma unroll
-        for (int u = 0; u < B; ++u) {
-            const uint32_t kf = k + B * (1 + FCU_L2PF) + u;
-            if (kf < cnt) prefetch_l2(&nbr[(size_t)kf * n + i]);
-        }
-#endif
-#pragma unroll
-        for (int u = 0; u < B; ++u)
-            if (k + u < cnt) use(f3(e[u].x, e[u].y, e[u].z), v[u]);
-#pragma unroll
-        for (int u = 0; u < B; ++u) e[u] = en[u];
-    }
-}
-
 struct PosKd {
     float4 p;
     float kd;
@@ -479,14 +439,14 @@ struct DensitySums {
 
 template <class KP>
 __device__ __forceinline__ float density_pair(const KP &P, DensitySums &d, F3 pos, F3 vel,
-                                              F3 x, float r2, float4 vj, F3 &gw) {
+                                              F3 x, float r2, float4 vj) {
     const float r = sqrtf(r2);
     const float q = r * P.inv_h;
     d.w_sum += kernel_q(P, q);
     const float wn = fmaxf(1.0f - q, 0.0f);
     d.rho_near += wn * wn * wn;
     const float gs = grad_scale(P, r, q);
-    gw = gs * x;
+    const F3 gw = gs * x;
     d.grad_sum = d.grad_sum + gw;
     d.grad_sq += dot(gw, gw);
     d.drho += dot(vel - xyz(vj), gw);
@@ -525,12 +485,8 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
                 const F3 x = pos - xyz(__ldg(&b.wpos[k]));
                 const float r2 = dot(x, x);
                 if (r2 >= P.support_sq) continue;
-                F3 gw;
-                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]), gw);
-                if (found < P.nbr_cap) {
-                    b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
-                    if (b.nbr_g) b.nbr_g[(size_t)found * n + i] = make_float4(gw.x, gw.y, gw.z, __uint_as_float(k));
-                }
+                const float gs = density_pair(P, d, pos, vel, x, r2, __ldg(&b.wvel[k]));
+                if (found < P.nbr_cap) b.nbr[(size_t)found * n + i] = make_uint2(k, __float_as_uint(gs));
                 found++;
             }
         }
@@ -647,15 +603,9 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
                     for (int u = 0; u < kP2; ++u) {
                         if (h + u < staged) {
                             const F3 x = pos - xyz(pj[u]);
-                            F3 gw;
-                            const float gs = density_pair(K, d, pos, vel, x, dot(x, x), vj[u], gw);
+                            const float gs = density_pair(K, d, pos, vel, x, dot(x, x), vj[u]);
                             const uint32_t idx = found + h + u;
-                            if (idx < cap) {
-                                b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
-                                if (!kB)
-                                    b.nbr_g[(size_t)idx * n + i] =
-                                        make_float4(gw.x, gw.y, gw.z, __uint_as_float(j[u]));
-                            }
+                            if (idx < cap) b.nbr[(size_t)idx * n + i] = make_uint2(j[u], __float_as_uint(gs));
                         }
                     }
                 }
@@ -944,17 +894,10 @@ __device__ __forceinline__ void den_kappa_at(const Geo &g, const SimBufs &b, uin
         const F3 vel = xyz(__ldg(&b.wvel[i]));
         const uint32_t cnt = __ldg(&b.nbr_n[i]);
         float drho = 0.0f;
-        if (!kB) {
-            // one box: the gradient list, one velocity record per neighbour
-            walk_grad<FCU_B_PV, float4>(
-                b.nbr_g, n, i, cnt, [&](uint32_t j) { return __ldg(&b.wvel[j]); },
-                [&](F3 gw, const float4 &v) { drho += dot(vel - xyz(v), gw); });
-        } else {
-            walk<FCU_B_PV, PosVel>(
-                b.nbr, n, i, cnt,
-                [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
-                [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
-        }
+        walk<FCU_B_PV, PosVel>(
+            b.nbr, n, i, cnt,
+            [&](uint32_t j) { return PosVel{__ldg(&b.wpos[j]), __ldg(&b.wvel[j])}; },
+            [&](float gs, const PosVel &q) { drho += dot(vel - xyz(q.v), pair_grad(gs, pos, q.p)); });
         const float rho = __ldg(&b.density[i]);
         drho = mass * drho + dot(vel, xyz(__ldg(&b.wgrad[i])));
         const float rho_star = rho + dt * drho;
@@ -974,66 +917,6 @@ __global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     den_kappa_at<kB>(g, b, i, i < g.n, slot, gate);
 }
-
-// ---- the batch's loop sweeps over a work list -------------------------------
-// Inside a tolerance loop only the boxes whose loop goes on are swept. The
-// loop's finishing kernel lists them (k_tol_finish: each active box with the
-// exclusive prefix of its tiles of kListTile consecutive slots), and these
-// persistent kernels walk that list: block after block takes the next tile,
-// finds its box by binary search over the prefix, and runs the same
-// per-slot body as the one-launch-per-sweep kernels. Boxes that stopped cost
-// nothing; the sums are those of the gated kernels, slot for slot.
-constexpr uint32_t kListTile = kSolveThreads;
-
-// Slot of this thread in work item w of list `which`; false for a lane past
-// its box's last slot (i is then that last slot).
-__device__ __forceinline__ bool work_slot(const Geo &g, int which, uint32_t nact, uint32_t w, uint32_t &i) {
-    const uint32_t *pre = g.wl_prefix[which];
-    uint32_t lo = 0, hi = nact;
-    while (hi - lo > 1u) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (pre[mid] <= w) lo = mid;
-        else hi = mid;
-    }
-    const uint32_t bx = g.wl_box[which][lo];
-    const uint32_t first = g.first[bx], cnt = g.box[bx].count;
-    i = first + (w - pre[lo]) * kListTile + threadIdx.x;
-    const bool live = i < first + cnt;
-    if (!live) i = first + cnt - 1u;
-    return live;
-}
-
-__global__ void __launch_bounds__(kListTile, kBatchKappaThreads / kListTile) k_apply_list(Geo g, SimBufs b,
-                                                                                       int add_pressure, int which) {
-    const uint32_t nact = *g.wl_nact[which];
-    const uint32_t total = nact ? g.wl_prefix[which][nact] : 0u;
-    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
-        uint32_t i;
-        if (work_slot(g, which, nact, w, i)) apply_at<true>(g, b, i, add_pressure, kGateNone);
-    }
-}
-
-__global__ void __launch_bounds__(kListTile, kBatchKappaThreads / kListTile) k_den_kappa_list(Geo g, SimBufs b,
-                                                                                           int slot, int which) {
-    const uint32_t nact = *g.wl_nact[which];
-    const uint32_t total = nact ? g.wl_prefix[which][nact] : 0u;
-    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
-        uint32_t i;
-        const bool live = work_slot(g, which, nact, w, i);
-        den_kappa_at<true>(g, b, i, live, slot, kGateNone);
-    }
-}
-
-__global__ void __launch_bounds__(kListTile, FCU_MINB) k_forces_div_list(Geo g, SimBufs b, int slot, int which) {
-    const uint32_t nact = *g.wl_nact[which];
-    const uint32_t total = nact ? g.wl_prefix[which][nact] : 0u;
-    for (uint32_t w = blockIdx.x; w < total; w += gridDim.x) {
-        uint32_t i;
-        const bool live = work_slot(g, which, nact, w, i);
-        forces_eval_body<true, true>(g, b, i, live, slot, kGateNone);
-    }
-}
-
 
 // ---- integrate (sim_solve.wgsl:709-756) ------------------------------------
 // With div_slot >= 0 (the fixed schedule) each box's first slot also records
@@ -1133,60 +1016,6 @@ __global__ void __launch_bounds__(256) k_tol_finish(Geo g, int which, int first,
     }
     any = __syncthreads_or(any);
     if (threadIdx.x == 0) cudaGraphSetConditional(handle, any ? 1u : 0u);
-    if (!g.wl_box[which]) return;
-    // the work list of the loop's next iteration: active boxes in box order
-    // with the exclusive prefix of their tiles (a block scan per chunk)
-    __shared__ uint32_t s_wc[8], s_wt[8];
-    __shared__ uint32_t s_carry_c, s_carry_t;
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    if (threadIdx.x == 0) {
-        s_carry_c = 0u;
-        s_carry_t = 0u;
-    }
-    __syncthreads();
-    for (uint32_t base = 0; base < g.nboxes; base += blockDim.x) {
-        const uint32_t bx = base + threadIdx.x;
-        uint32_t act = 0, til = 0;
-        if (bx < g.nboxes) {
-            const DevSolve &sv = g.solve[bx];
-            act = (which == 0 ? sv.div_active : sv.den_active) ? 1u : 0u;
-            til = act ? (g.box[bx].count + kListTile - 1u) / kListTile : 0u;
-        }
-        uint32_t c = act, t = til;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t cu = __shfl_up_sync(0xffffffffu, c, o), tu = __shfl_up_sync(0xffffffffu, t, o);
-            if (lane >= (uint32_t)o) {
-                c += cu;
-                t += tu;
-            }
-        }
-        if (lane == 31) {
-            s_wc[warp] = c;
-            s_wt[warp] = t;
-        }
-        __syncthreads();
-        uint32_t oc = s_carry_c, ot = s_carry_t;
-        for (uint32_t w = 0; w < warp; ++w) {
-            oc += s_wc[w];
-            ot += s_wt[w];
-        }
-        if (act) {
-            g.wl_box[which][oc + c - 1u] = bx;
-            g.wl_prefix[which][oc + c - 1u] = ot + t - til;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0)
-            for (uint32_t w = 0; w < nw; ++w) {
-                s_carry_c += s_wc[w];
-                s_carry_t += s_wt[w];
-            }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        g.wl_prefix[which][s_carry_c] = s_carry_t;
-        *g.wl_nact[which] = s_carry_c;
-    }
 }
 
 // ---- reduce_stats (sim_solve.wgsl:800-874) ---------------------------------
@@ -1491,30 +1320,6 @@ void launch_forces_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot,
 }
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b) {
     FCU_SWEEP(k_forces_apply, kTuneForcesApply, kSolveThreads, g, b);
-}
-// The persistent loop sweeps over a batch's work list: one wave of resident
-// kListTile-thread blocks (the list's length is only known on the device),
-// each striding over the tiles, so no block waits for a second wave.
-template <class K>
-uint32_t resident_blocks(K kernel) {
-    int dev = 0, sms = 0, per = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, (int)kListTile, 0);
-    const uint32_t n = (uint32_t)(sms > 0 ? sms : 1) * (uint32_t)(per > 0 ? per : 1);
-    return n;
-}
-void launch_apply_list(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int which) {
-    static const uint32_t blocks = resident_blocks(k_apply_list);
-    k_apply_list<<<blocks, kListTile, 0, s>>>(g, b, add_pressure ? 1 : 0, which);
-}
-void launch_den_kappa_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which) {
-    static const uint32_t blocks = resident_blocks(k_den_kappa_list);
-    k_den_kappa_list<<<blocks, kListTile, 0, s>>>(g, b, slot, which);
-}
-void launch_forces_div_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which) {
-    static const uint32_t blocks = resident_blocks(k_forces_div_list);
-    k_forces_div_list<<<blocks, kListTile, 0, s>>>(g, b, slot, which);
 }
 void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate) {
     FCU_SWEEP(k_den_kappa, kTuneDenKappa, kSolveThreads, g, b, slot, gate);

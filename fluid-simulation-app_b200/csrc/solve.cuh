@@ -5,11 +5,6 @@
 
 namespace fcu {
 
-// FCU_BATCH_LIST 1: a batch's tolerance loops sweep only their active boxes
-// through work lists (persistent list kernels); 0: gated full launches.
-#ifndef FCU_BATCH_LIST
-#define FCU_BATCH_LIST 0
-#endif
 
 // Device pointers of the particle state and scratch: one box, or a batch of
 // boxes laid end to end (box b owns slots first[b] .. first[b] + count - 1 in
@@ -39,12 +34,6 @@ struct SimBufs {
     // square root and the division density_div already did.
     uint2 *nbr;
     uint32_t *nbr_n;
-    // One box only (null in a batch): the same entries as (kernel gradient
-    // xyz, slot bits in w), which density_div also writes, so den_kappa reads
-    // each neighbour's velocity and nothing else: 16 more bytes an entry
-    // written once, one 16-byte gather fewer per entry in every density
-    // prediction (0.205 -> 0.176 ms a launch on the 1M workload).
-    float4 *nbr_g;
     // tracers (one box)
     uint32_t *tracers;  // 2 words each
     int32_t *vel_grid;  // 4 per cell, atomic sums
@@ -84,12 +73,6 @@ struct Geo {
     const DevStep *st;                       // [nboxes] this substep's Step blocks
     uint32_t n;                              // particles in all boxes
     uint32_t nboxes;
-    // A batch's tolerance-loop work lists ([0] divergence, [1] density),
-    // written by the loop's finishing kernel: the active boxes, the exclusive
-    // prefix of their tiles ([count + 1]) and the count. Null: none kept.
-    uint32_t *wl_box[2];
-    uint32_t *wl_prefix[2];
-    uint32_t *wl_nact[2];
 };
 
 constexpr int kSolveThreads = 128;
@@ -110,12 +93,6 @@ void launch_forces_eval(cudaStream_t s, const Geo &g, const SimBufs &b);
 // loop has stopped.
 void launch_forces_div(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate);
 void launch_forces_apply(cudaStream_t s, const Geo &g, const SimBufs &b);
-// The batch's loop sweeps over the active boxes only (Geo work lists): what
-// apply / den_kappa / forces_div with the loop's gate compute, from a fixed
-// grid of persistent blocks.
-void launch_apply_list(cudaStream_t s, const Geo &g, const SimBufs &b, bool add_pressure, int which);
-void launch_den_kappa_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which);
-void launch_forces_div_list(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int which);
 
 void launch_den_kappa(cudaStream_t s, const Geo &g, const SimBufs &b, int slot, int gate);
 // div_slot >= 0: record each box's residuals from those accumulator slots
