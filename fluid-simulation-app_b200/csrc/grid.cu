@@ -377,28 +377,49 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
     __syncthreads();
     const uint32_t tile = s_tile;
 
-    const uint64_t wbase = (uint64_t)tile * kSortTile + (uint64_t)warp * (32 * kSortItems);
+    // Indices fit 32 bits: the last tile ends at ceil(n / kSortTile) *
+    // kSortTile <= 2^32 for any 32-bit n. A full tile (every tile but the
+    // last) takes the loads and ballots without per-element bounds.
+    const uint32_t wbase = tile * kSortTile + warp * (32 * kSortItems);
+    const bool full = (uint64_t)(tile + 1) * kSortTile <= n;
     const uint32_t lt = lanemask_lt();
     uint32_t key[kSortItems], rank[kSortItems];
+    if (full) {
 #pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
-        const uint64_t i = wbase + (uint64_t)r * 32 + lane;
-        key[r] = i < n ? __ldg(&keys_in[i]) : 0u;
+        for (int r = 0; r < kSortItems; ++r) key[r] = __ldg(&keys_in[wbase + r * 32 + lane]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < kSortItems; ++r) {
+            const uint32_t i = wbase + r * 32 + lane;
+            key[r] = i < n ? __ldg(&keys_in[i]) : 0u;
+        }
     }
     // every round's digit peers first (ballots and registers only), then the
     // rounds in order: the leader of each group of peers adds the group to
     // the warp's count of its digit and hands the old count to the group
+    if (full) {
 #pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
-        const bool live = wbase + (uint64_t)r * 32 + lane < n;
-        const uint32_t act = __ballot_sync(0xffffffffu, live);
-        const uint32_t d = (key[r] >> shift) & (kRadix - 1);
+        for (int r = 0; r < kSortItems; ++r) {
+            const uint32_t d = (key[r] >> shift) & (kRadix - 1);
 #if FCU_SORT_MATCH
-        const uint32_t pe = live ? __match_any_sync(act, d) : 0u;
+            rank[r] = __match_any_sync(0xffffffffu, d);
 #else
-        const uint32_t pe = digit_peers(act, d);
+            rank[r] = digit_peers(0xffffffffu, d);
 #endif
-        rank[r] = live ? pe : 0u;  // a live lane is its own peer, so nonzero
+        }
+    } else {
+#pragma unroll
+        for (int r = 0; r < kSortItems; ++r) {
+            const bool live = wbase + r * 32 + lane < n;
+            const uint32_t act = __ballot_sync(0xffffffffu, live);
+            const uint32_t d = (key[r] >> shift) & (kRadix - 1);
+#if FCU_SORT_MATCH
+            const uint32_t pe = live ? __match_any_sync(act, d) : 0u;
+#else
+            const uint32_t pe = digit_peers(act, d);
+#endif
+            rank[r] = live ? pe : 0u;  // a live lane is its own peer, so nonzero
+        }
     }
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
@@ -474,17 +495,17 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        const uint64_t i = wbase + (uint64_t)r * 32 + lane;
-        if (i < n) {
+        const uint32_t i = wbase + r * 32 + lane;
+        if (full || i < n) {
             const uint32_t d = (key[r] >> shift) & (kRadix - 1);
             const uint32_t at = s_start[d] + s_hist[warp][d] + rank[r];
             s_key[at] = key[r];
-            s_val[at] = vals_in ? __ldg(&vals_in[i]) : (uint32_t)i;
+            s_val[at] = vals_in ? __ldg(&vals_in[i]) : i;
         }
     }
     __syncthreads();
-    const uint64_t tbase = (uint64_t)tile * kSortTile;
-    const uint32_t count = (uint32_t)(n - tbase < kSortTile ? n - tbase : kSortTile);
+    const uint32_t tbase = tile * kSortTile;
+    const uint32_t count = full ? kSortTile : n - tbase;
     for (uint32_t j = threadIdx.x; j < count; j += kSortThreads) {
         const uint32_t k = s_key[j];
         const uint32_t d = (k >> shift) & (kRadix - 1);
