@@ -68,12 +68,12 @@ ALGO_BYTES = {"grid": 20.0, "gather": 116.0, "density_div": 44.0, "div_kappa": 2
               "den_kappa": 36.0, "den_apply": 36.0, "integrate": 120.0}
 # DRAM bytes (read + write) per particle per launch: a constant taken from
 # one ncu capture of each kernel on this workload at its full 1,048,576
-# particles (dram__bytes_read.sum + dram__bytes_write.sum), not measured by
-# this script; a kernel change calls for a new capture.
-NCU_TRAFFIC_PER_PARTICLE = {"den_kappa": (583.2e6 + 19.4e6) / 1048576,
-                            "den_apply": (604.1e6 + 15.5e6) / 1048576,
-                            "div_apply": (604.1e6 + 15.5e6) / 1048576,
-                            "density_div": (71.9e6 + 505.6e6) / 1048576}
+# particles, on the state after the benchmark's 25 frames
+# (dram__bytes_read.sum + dram__bytes_write.sum), not measured by this
+# script; a kernel change calls for a new capture.
+NCU_TRAFFIC_PER_PARTICLE = {"density_div": (100.93e6 + 329.28e6) / 1048576,
+                            "forces_eval": (415.34e6 + 37.60e6) / 1048576,
+                            "den_kappa": (423.84e6 + 16.27e6) / 1048576}
 
 
 def workload_config(w, n):
