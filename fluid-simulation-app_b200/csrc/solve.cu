@@ -655,6 +655,59 @@ __device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
     return (gate == kGateDiv ? sv.div_active : sv.den_active) == 0u;
 }
 
+// ---- threads ordered by neighbour count -------------------------------------
+// A list sweep's warp runs as many iterations as its longest list, so lanes
+// whose particles have fewer neighbours idle. A block can hand its slots to
+// its threads in order of list length instead (a counting sort of the
+// block's slots by nbr_n in shared memory), so each warp holds particles of
+// similar counts. Which thread computes a particle changes nothing in its
+// sums, so the results are the same bits. Returns this thread's slot, or
+// g.n when the block has fewer slots than threads.
+#ifndef FCU_SORTED_FORCES
+#define FCU_SORTED_FORCES 0
+#endif
+#ifndef FCU_SORTED_KAPPA
+#define FCU_SORTED_KAPPA 0
+#endif
+#if FCU_SORTED_FORCES || FCU_SORTED_KAPPA
+constexpr int kCountBins = 64;  // nbr_n / 2, the last bin open-ended
+
+template <int TPB>
+__device__ __forceinline__ uint32_t slot_by_count(const SimBufs &b, uint32_t n) {
+    __shared__ uint32_t s_bin[kCountBins];
+    __shared__ uint32_t s_slot[TPB];
+    const uint32_t base = blockIdx.x * TPB, tid = threadIdx.x;
+    const uint32_t i0 = base + tid;
+    const bool live = i0 < n;
+    if (tid < (uint32_t)kCountBins) s_bin[tid] = 0u;
+    __syncthreads();
+    uint32_t bin = 0, rank = 0;
+    if (live) {
+        const uint32_t c = __ldg(&b.nbr_n[i0]) >> 1;
+        bin = c < (uint32_t)kCountBins ? c : (uint32_t)kCountBins - 1u;
+        rank = atomicAdd(&s_bin[bin], 1u);
+    }
+    __syncthreads();
+    if (tid < 32u) {  // exclusive scan of the 64 bins, two a lane
+        const uint32_t a0 = s_bin[2 * tid], a1 = s_bin[2 * tid + 1];
+        uint32_t x = a0 + a1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (tid >= (uint32_t)o) x += y;
+        }
+        const uint32_t excl = x - a0 - a1;
+        s_bin[2 * tid] = excl;
+        s_bin[2 * tid + 1] = excl + a0;
+    }
+    __syncthreads();
+    if (live) s_slot[s_bin[bin] + rank] = i0;
+    __syncthreads();
+    const uint32_t count = n > base ? (n - base < (uint32_t)TPB ? n - base : (uint32_t)TPB) : 0u;
+    return tid < count ? s_slot[tid] : n;
+}
+#endif
+
 // ---- divergence predictor for a later divergence iteration ---------------
 // density_div's divergence sums again over the list, with this
 // iteration's velocities.
@@ -724,7 +777,11 @@ __device__ __forceinline__ void apply_at(const Geo &g, const SimBufs &b, uint32_
 
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure, int gate) {
+#if FCU_SORTED_KAPPA
+    const uint32_t i = slot_by_count<TPB>(b, g.n);
+#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#endif
     if (i < g.n) apply_at<kB>(g, b, i, add_pressure, gate);
 }
 
@@ -821,12 +878,20 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
 
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
+#if FCU_SORTED_FORCES
+    const uint32_t i = slot_by_count<TPB>(b, g.n);
+#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#endif
     forces_eval_body<kB, false>(g, b, i, i < g.n, slot, gate);
 }
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
+#if FCU_SORTED_FORCES
+    const uint32_t i = slot_by_count<TPB>(b, g.n);
+#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#endif
     forces_eval_body<kB, true>(g, b, i, i < g.n, slot, gate);
 }
 
@@ -854,7 +919,11 @@ __device__ __forceinline__ F3 fingers(const FluidStep &st, F3 pos, F3 v) {
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_apply(Geo g, SimBufs b) {
     const uint32_t n = g.n;
+#if FCU_SORTED_FORCES
+    const uint32_t i = slot_by_count<TPB>(b, n);
+#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#endif
     if (i >= n) return;
     const uint32_t bi = box_index<kB>(g, i);
     const float mass = params_of<kB>(g, bi).mass;
@@ -914,7 +983,11 @@ __device__ __forceinline__ void den_kappa_at(const Geo &g, const SimBufs &b, uin
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
+#if FCU_SORTED_KAPPA
+    const uint32_t i = slot_by_count<TPB>(b, g.n);
+#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+#endif
     den_kappa_at<kB>(g, b, i, i < g.n, slot, gate);
 }
 
