@@ -662,14 +662,15 @@ __device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
 // block's slots by nbr_n in shared memory), so each warp holds particles of
 // similar counts. Which thread computes a particle changes nothing in its
 // sums, so the results are the same bits. Returns this thread's slot, or
-// g.n when the block has fewer slots than threads.
+// g.n when the block has fewer slots than threads. forces_eval, issue-bound
+// on its per-pair divisions, gains (0.474 -> 0.439 ms on the 1M workload);
+// the L1-bound sweeps (apply 0.108 -> 0.125, forces_apply 0.10 -> 0.127 ms)
+// lose more on their scattered own-record and list loads, and keep slot
+// order.
 #ifndef FCU_SORTED_FORCES
-#define FCU_SORTED_FORCES 0
+#define FCU_SORTED_FORCES 1
 #endif
-#ifndef FCU_SORTED_KAPPA
-#define FCU_SORTED_KAPPA 0
-#endif
-#if FCU_SORTED_FORCES || FCU_SORTED_KAPPA
+#if FCU_SORTED_FORCES
 constexpr int kCountBins = 64;  // nbr_n / 2, the last bin open-ended
 
 template <int TPB>
@@ -777,11 +778,7 @@ __device__ __forceinline__ void apply_at(const Geo &g, const SimBufs &b, uint32_
 
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_apply(Geo g, SimBufs b, int add_pressure, int gate) {
-#if FCU_SORTED_KAPPA
-    const uint32_t i = slot_by_count<TPB>(b, g.n);
-#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-#endif
     if (i < g.n) apply_at<kB>(g, b, i, add_pressure, gate);
 }
 
@@ -919,11 +916,7 @@ __device__ __forceinline__ F3 fingers(const FluidStep &st, F3 pos, F3 v) {
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_apply(Geo g, SimBufs b) {
     const uint32_t n = g.n;
-#if FCU_SORTED_FORCES
-    const uint32_t i = slot_by_count<TPB>(b, n);
-#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-#endif
     if (i >= n) return;
     const uint32_t bi = box_index<kB>(g, i);
     const float mass = params_of<kB>(g, bi).mass;
@@ -983,11 +976,7 @@ __device__ __forceinline__ void den_kappa_at(const Geo &g, const SimBufs &b, uin
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, kB ? kBatchKappaThreads / TPB : FCU_MINB_KAPPA) k_den_kappa(Geo g, SimBufs b, int slot,
                                                                        int gate) {
-#if FCU_SORTED_KAPPA
-    const uint32_t i = slot_by_count<TPB>(b, g.n);
-#else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-#endif
     den_kappa_at<kB>(g, b, i, i < g.n, slot, gate);
 }
 
