@@ -345,6 +345,9 @@ __global__ void __launch_bounds__(256) k_gather(SimBufs b, uint32_t n) {
     b.wpp[k] = __ldg(&b.pp[i]);
     b.wtemp[k] = __ldg(&b.temp[i]);
     b.wid[k] = __ldg(&b.id[i]);
+#if FCU_SORTED_DENSITY
+    b.nbr_prev[k] = __ldg(&b.nbr_n[i]);  // the resting slot is the last substep's working slot
+#endif
 }
 
 // Per-box views of a Geo. kB (batch) is a template flag so the one-box
@@ -453,6 +456,65 @@ __device__ __forceinline__ float density_pair(const KP &P, DensitySums &d, F3 po
     return gs;
 }
 
+// ---- threads ordered by neighbour count -------------------------------------
+// A list sweep's warp runs as many iterations as its longest list, so lanes
+// whose particles have fewer neighbours idle. A block can hand its slots to
+// its threads in order of list length instead (a counting sort of the
+// block's slots by nbr_n in shared memory), so each warp holds particles of
+// similar counts. Which thread computes a particle changes nothing in its
+// sums, so the results are the same bits. Returns this thread's slot, or
+// g.n when the block has fewer slots than threads. forces_eval, issue-bound
+// on its per-pair divisions, gains (0.474 -> 0.439 ms on the 1M workload);
+// the L1-bound sweeps (apply 0.108 -> 0.125, forces_apply 0.10 -> 0.127 ms)
+// lose more on their scattered own-record and list loads, and keep slot
+// order.
+#ifndef FCU_SORTED_FORCES
+#define FCU_SORTED_FORCES 1
+#endif
+// FCU_SORTED_DENSITY: density_div orders its threads by each particle's
+// neighbour count of the previous substep (gathered with the particle).
+#ifndef FCU_SORTED_DENSITY
+#define FCU_SORTED_DENSITY 0
+#endif
+#if FCU_SORTED_FORCES || FCU_SORTED_DENSITY
+constexpr int kCountBins = 64;  // nbr_n / 2, the last bin open-ended
+
+template <int TPB>
+__device__ __forceinline__ uint32_t slot_by_count(const uint32_t *__restrict__ counts, uint32_t n) {
+    __shared__ uint32_t s_bin[kCountBins];
+    __shared__ uint32_t s_slot[TPB];
+    const uint32_t base = blockIdx.x * TPB, tid = threadIdx.x;
+    const uint32_t i0 = base + tid;
+    const bool live = i0 < n;
+    if (tid < (uint32_t)kCountBins) s_bin[tid] = 0u;
+    __syncthreads();
+    uint32_t bin = 0, rank = 0;
+    if (live) {
+        const uint32_t c = __ldg(&counts[i0]) >> 1;
+        bin = c < (uint32_t)kCountBins ? c : (uint32_t)kCountBins - 1u;
+        rank = atomicAdd(&s_bin[bin], 1u);
+    }
+    __syncthreads();
+    if (tid < 32u) {  // exclusive scan of the 64 bins, two a lane
+        const uint32_t a0 = s_bin[2 * tid], a1 = s_bin[2 * tid + 1];
+        uint32_t x = a0 + a1;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (tid >= (uint32_t)o) x += y;
+        }
+        const uint32_t excl = x - a0 - a1;
+        s_bin[2 * tid] = excl;
+        s_bin[2 * tid + 1] = excl + a0;
+    }
+    __syncthreads();
+    if (live) s_slot[s_bin[bin] + rank] = i0;
+    __syncthreads();
+    const uint32_t count = n > base ? (n - base < (uint32_t)TPB ? n - base : (uint32_t)TPB) : 0u;
+    return tid < count ? s_slot[tid] : n;
+}
+#endif
+
 // ---- density_div (sim_solve.wgsl:411-518) --------------------------------
 // One thread per particle, in rounds of two phases. Phase 1: the thread walks
 // its own stencil candidates in order and stages each hit as a (row, offset)
@@ -501,7 +563,11 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
     __shared__ uint32_t s_end[9][TPB];
     const uint32_t n = g.n;
     const uint32_t tid = threadIdx.x;
+#if FCU_SORTED_DENSITY
+    const uint32_t i = slot_by_count<TPB>(b.nbr_prev, n);
+#else
     const uint32_t i = blockIdx.x * blockDim.x + tid;
+#endif
     const bool live = i < n;
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;
@@ -655,59 +721,6 @@ __device__ __forceinline__ bool gated_out(const Geo &g, uint32_t bi, int gate) {
     return (gate == kGateDiv ? sv.div_active : sv.den_active) == 0u;
 }
 
-// ---- threads ordered by neighbour count -------------------------------------
-// A list sweep's warp runs as many iterations as its longest list, so lanes
-// whose particles have fewer neighbours idle. A block can hand its slots to
-// its threads in order of list length instead (a counting sort of the
-// block's slots by nbr_n in shared memory), so each warp holds particles of
-// similar counts. Which thread computes a particle changes nothing in its
-// sums, so the results are the same bits. Returns this thread's slot, or
-// g.n when the block has fewer slots than threads. forces_eval, issue-bound
-// on its per-pair divisions, gains (0.474 -> 0.439 ms on the 1M workload);
-// the L1-bound sweeps (apply 0.108 -> 0.125, forces_apply 0.10 -> 0.127 ms)
-// lose more on their scattered own-record and list loads, and keep slot
-// order.
-#ifndef FCU_SORTED_FORCES
-#define FCU_SORTED_FORCES 1
-#endif
-#if FCU_SORTED_FORCES
-constexpr int kCountBins = 64;  // nbr_n / 2, the last bin open-ended
-
-template <int TPB>
-__device__ __forceinline__ uint32_t slot_by_count(const SimBufs &b, uint32_t n) {
-    __shared__ uint32_t s_bin[kCountBins];
-    __shared__ uint32_t s_slot[TPB];
-    const uint32_t base = blockIdx.x * TPB, tid = threadIdx.x;
-    const uint32_t i0 = base + tid;
-    const bool live = i0 < n;
-    if (tid < (uint32_t)kCountBins) s_bin[tid] = 0u;
-    __syncthreads();
-    uint32_t bin = 0, rank = 0;
-    if (live) {
-        const uint32_t c = __ldg(&b.nbr_n[i0]) >> 1;
-        bin = c < (uint32_t)kCountBins ? c : (uint32_t)kCountBins - 1u;
-        rank = atomicAdd(&s_bin[bin], 1u);
-    }
-    __syncthreads();
-    if (tid < 32u) {  // exclusive scan of the 64 bins, two a lane
-        const uint32_t a0 = s_bin[2 * tid], a1 = s_bin[2 * tid + 1];
-        uint32_t x = a0 + a1;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if (tid >= (uint32_t)o) x += y;
-        }
-        const uint32_t excl = x - a0 - a1;
-        s_bin[2 * tid] = excl;
-        s_bin[2 * tid + 1] = excl + a0;
-    }
-    __syncthreads();
-    if (live) s_slot[s_bin[bin] + rank] = i0;
-    __syncthreads();
-    const uint32_t count = n > base ? (n - base < (uint32_t)TPB ? n - base : (uint32_t)TPB) : 0u;
-    return tid < count ? s_slot[tid] : n;
-}
-#endif
 
 // ---- divergence predictor for a later divergence iteration ---------------
 // density_div's divergence sums again over the list, with this
@@ -876,7 +889,7 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
 #if FCU_SORTED_FORCES
-    const uint32_t i = slot_by_count<TPB>(b, g.n);
+    const uint32_t i = slot_by_count<TPB>(b.nbr_n, g.n);
 #else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 #endif
@@ -885,7 +898,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b
 template <bool kB, int TPB>
 __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
 #if FCU_SORTED_FORCES
-    const uint32_t i = slot_by_count<TPB>(b, g.n);
+    const uint32_t i = slot_by_count<TPB>(b.nbr_n, g.n);
 #else
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
 #endif
