@@ -352,7 +352,6 @@ int32_t batch_create_into(FluidBatch *s, const FluidSimConfig *boxes, uint32_t n
     BK(s->alloc(&b.wgrad, n));
     BK(s->alloc(&b.nbr, n * s->common.nbr_cap));
     BK(s->alloc(&b.nbr_n, n));
-    BK(s->alloc(&b.nbr_prev, n));
     BK(s->alloc(&b.stats_part, nb * s->chunks * 12));
     BK(s->alloc(&b.stats_acc, nb));
     BK(s->alloc(&b.stats, nb * 16));

@@ -674,7 +674,6 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(s->alloc(&b.wgrad, n));
     CK(s->alloc(&b.nbr, n * cfg->nbr_cap));
     CK(s->alloc(&b.nbr_n, n));
-    CK(s->alloc(&b.nbr_prev, n));
     CK(s->alloc(&b.tracers, 2 * (size_t)(s->ntr > 0 ? s->ntr : 1)));
     CK(s->alloc(&b.vel_grid, 4 * C));
     CK(s->alloc(&b.vel_flat, C));

@@ -345,9 +345,6 @@ __global__ void __launch_bounds__(256) k_gather(SimBufs b, uint32_t n) {
     b.wpp[k] = __ldg(&b.pp[i]);
     b.wtemp[k] = __ldg(&b.temp[i]);
     b.wid[k] = __ldg(&b.id[i]);
-#if FCU_SORTED_DENSITY
-    b.nbr_prev[k] = __ldg(&b.nbr_n[i]);  // the resting slot is the last substep's working slot
-#endif
 }
 
 // Per-box views of a Geo. kB (batch) is a template flag so the one-box
@@ -467,16 +464,12 @@ __device__ __forceinline__ float density_pair(const KP &P, DensitySums &d, F3 po
 // on its per-pair divisions, gains (0.474 -> 0.439 ms on the 1M workload);
 // the L1-bound sweeps (apply 0.108 -> 0.125, forces_apply 0.10 -> 0.127 ms)
 // lose more on their scattered own-record and list loads, and keep slot
-// order.
+// order, and density_div ordered by each particle's neighbour count of the
+// last substep measured slower too (0.643 -> 0.672 ms).
 #ifndef FCU_SORTED_FORCES
 #define FCU_SORTED_FORCES 1
 #endif
-// FCU_SORTED_DENSITY: density_div orders its threads by each particle's
-// neighbour count of the previous substep (gathered with the particle).
-#ifndef FCU_SORTED_DENSITY
-#define FCU_SORTED_DENSITY 0
-#endif
-#if FCU_SORTED_FORCES || FCU_SORTED_DENSITY
+#if FCU_SORTED_FORCES
 constexpr int kCountBins = 64;  // nbr_n / 2, the last bin open-ended
 
 template <int TPB>
@@ -563,11 +556,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
     __shared__ uint32_t s_end[9][TPB];
     const uint32_t n = g.n;
     const uint32_t tid = threadIdx.x;
-#if FCU_SORTED_DENSITY
-    const uint32_t i = slot_by_count<TPB>(b.nbr_prev, n);
-#else
     const uint32_t i = blockIdx.x * blockDim.x + tid;
-#endif
     const bool live = i < n;
     const uint32_t bi = box_index<kB>(g, live ? i : n - 1);
     unsigned long long term = 0;

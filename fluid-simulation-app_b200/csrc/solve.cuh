@@ -34,7 +34,6 @@ struct SimBufs {
     // square root and the division density_div already did.
     uint2 *nbr;
     uint32_t *nbr_n;
-    uint32_t *nbr_prev;  // each working slot's neighbour count of the last substep (FCU_SORTED_DENSITY)
     // tracers (one box)
     uint32_t *tracers;  // 2 words each
     int32_t *vel_grid;  // 4 per cell, atomic sums
