@@ -362,7 +362,7 @@ def cuda_arm(args):
                                            "workload (dram__bytes_read.sum + dram__bytes_write.sum), "
                                            "not measured in this run",
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
-                         "algorithmic": "own records, list-free (36 B per particle for the kappa sweeps)",
+                         "algorithmic": f"own records, list-free ({ALGO_BYTES[dom]:.0f} B per particle for {dom})",
                          "mean_neighbours": mean_nbrs,
                          "achieved_with_list": (ALGO_BYTES[dom] + list_bytes) * n / (avg_ms / 1000.0) / 1e9,
                          "frac_with_list": (ALGO_BYTES[dom] + list_bytes) * n / (avg_ms / 1000.0) / 1e9 / peak,
