@@ -261,7 +261,7 @@ def cuda_arm(args):
     # step, forces pair, first density prediction and its residual step,
     # integrate; 3 per loop iteration; per frame stats (2) and tracers (3).
     passes = 1
-    cells = sim.cells
+    cells = sim.keyspace
     while (cells - 1) >> (8 * passes):
         passes += 1
     fixed = 2 + passes + 1 + 2 + 4 + 1

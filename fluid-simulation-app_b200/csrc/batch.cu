@@ -101,7 +101,7 @@ struct FluidBatch {
         for (int k = 0; k < 8; ++k) g.tpb[k] = tpb[k];
         return g;
     }
-    BoxKeys keys() const { return BoxKeys{d_box_of, d_box, d_cell_base, nboxes}; }
+    BoxKeys keys() const { return BoxKeys{d_box_of, d_box, d_cell_base, nboxes, kSimSlabs}; }
 
     template <class T>
     cudaError_t alloc(T **p, size_t cnt) {
@@ -297,9 +297,10 @@ int32_t batch_create_into(FluidBatch *s, const FluidSimConfig *boxes, uint32_t n
         const uint64_t c = (uint64_t)s->P[bx].dims[0] * s->P[bx].dims[1] * s->P[bx].dims[2];
         s->first.push_back((uint32_t)n64);
         s->count.push_back((uint32_t)cnt);
+        // grid keys: each box's cells * kSimSlabs keys above the earlier boxes'
         s->cell_base.push_back((uint32_t)cells64);
         n64 += cnt;
-        cells64 += c;
+        cells64 += c * kSimSlabs;
         if (n64 > 0x0fffffffull) return report_error(FLUID_ERR_ARG, "a batch holds at most 2^28-1 particles");
         if (cells64 >= 0xffffffffull) return report_error(FLUID_ERR_ARG, "the batch's grids have too many cells");
         pos.insert(pos.end(), p.begin(), p.end());

@@ -113,6 +113,24 @@ __device__ __forceinline__ uint32_t axis_cell(float v, float mn, float cell, uin
     return u < dim - 1u ? u : dim - 1u;
 }
 
+// Slabs per cell along x in a simulation's grid keys (GridGeom::slabs).
+#ifndef FCU_SLABS
+#define FCU_SLABS 1
+#endif
+constexpr uint32_t kSimSlabs = FCU_SLABS;
+
+// Slab of coordinate v inside its cell c of one axis: the cell cut into
+// `slabs` equal slabs across the axis, 0 .. slabs - 1, counted by threshold
+// tests (a NaN offset, or one below the cell, gives 0; one past it, the last
+// slab). Monotonic in v for a fixed c, and with the cell, so the key
+// cell * slabs + slab orders an axis like its coordinate.
+__device__ __forceinline__ uint32_t axis_slab(float v, float mn, float cell, uint32_t c, uint32_t slabs) {
+    const float off = v - (mn + (float)c * cell);
+    uint32_t s = 0;
+    for (uint32_t k = 1; k < slabs; ++k) s += off >= cell * ((float)k / (float)slabs) ? 1u : 0u;
+    return s;
+}
+
 // Fixed-point scale of the residual sums: 2^-28 per unit, each term capped
 // at 16, so a 64-bit sum over 2^32 particles cannot wrap.
 constexpr double kFixedScale = 268435456.0;

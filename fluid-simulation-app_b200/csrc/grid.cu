@@ -124,6 +124,7 @@ __global__ void __launch_bounds__(kSortThreads) k_cell_keys(const float4 *__rest
                 const uint32_t cy = axis_cell(p[u].y, g.min[1], g.cell, g.dims[1]);
                 const uint32_t cz = axis_cell(p[u].z, g.min[2], g.cell, g.dims[2]);
                 key = (cz * g.dims[1] + cy) * g.dims[0] + cx;
+                if (g.slabs > 1) key = key * g.slabs + axis_slab(p[u].x, g.min[0], g.cell, cx, g.slabs);
                 keys[i] = key;
             }
             count_digits(h, passes, live, key);
@@ -163,7 +164,10 @@ __global__ void __launch_bounds__(kSortThreads) k_box_keys(const float4 *__restr
             const uint32_t cx = axis_cell(p.x, __ldg(&P->box_min[0]), cell, dx);
             const uint32_t cy = axis_cell(p.y, __ldg(&P->box_min[1]), cell, dy);
             const uint32_t cz = axis_cell(p.z, __ldg(&P->box_min[2]), cell, dz);
-            key = __ldg(&bk.cell_base[b]) + (cz * dy + cy) * dx + cx;
+            key = (cz * dy + cy) * dx + cx;
+            if (bk.slabs > 1)
+                key = key * bk.slabs + axis_slab(p.x, __ldg(&P->box_min[0]), cell, cx, bk.slabs);
+            key += __ldg(&bk.cell_base[b]);
             keys[i] = key;
         }
         count_digits(h, passes, live, key);

@@ -9,6 +9,9 @@ struct GridGeom {
     float min[3];
     float cell;
     uint32_t dims[3];
+    // slabs > 1: each cell is cut into that many slabs along x and the key
+    // is cell * slabs + slab, so a cell's slots are in slab order
+    uint32_t slabs = 1;
 };
 
 constexpr int kScanThreads = 256;
@@ -65,13 +68,14 @@ int32_t read_build_status(const uint32_t *err, cudaStream_t stream, const char *
 cudaError_t enqueue_stalled_radix_pass(const GridWork &w, cudaStream_t stream);
 
 // A batch of boxes sharing one grid: slot i belongs to box box_of[i], whose
-// cells are keys cell_base[b] .. cell_base[b] + its cells - 1 (the boxes'
-// cell ranges laid end to end, in box order).
+// keys are cell_base[b] .. cell_base[b] + its cells * slabs - 1 (the boxes'
+// key ranges laid end to end, in box order; key cell * slabs + x slab).
 struct BoxKeys {
     const uint16_t *box_of;     // [n]
     const DevParams *box;       // [nboxes]
     const uint32_t *cell_base;  // [nboxes]
     uint32_t nboxes;
+    uint32_t slabs = 1;
 };
 
 // Enqueues keys -> stable radix sort -> starts on `stream`. `keys` receives

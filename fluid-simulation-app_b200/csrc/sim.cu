@@ -100,6 +100,7 @@ struct FluidSim {
     FluidSimConfig cfg{};
     DevParams P{};
     uint32_t n = 0, cells = 0, ntr = 0;
+    uint32_t keyspace = 0;  // grid keys: cells * kSimSlabs
     int device = 0;
     cudaStream_t stream = nullptr;
     SimBufs b{};
@@ -290,6 +291,7 @@ GridGeom geom_of(const DevParams &P) {
         g.dims[i] = P.dims[i];
     }
     g.cell = P.cell;
+    g.slabs = kSimSlabs;
     return g;
 }
 
@@ -639,6 +641,8 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     const uint64_t cells64 = (uint64_t)s->P.dims[0] * s->P.dims[1] * s->P.dims[2];
     if (cells64 >= 0xffffffffull) return fail(FLUID_ERR_ARG, "grid has too many cells");
     s->cells = (uint32_t)cells64;
+    if (cells64 * kSimSlabs >= 0xffffffffull) return fail(FLUID_ERR_ARG, "grid has too many cells");
+    s->keyspace = (uint32_t)(cells64 * kSimSlabs);
     s->ntr = cfg->tracers;
     if ((uint64_t)s->n * cfg->nbr_cap > (1ull << 40)) return fail(FLUID_ERR_ARG, "neighbour lists too large");
 
@@ -658,7 +662,7 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(s->alloc(&b.wtemp, n));
     CK(s->alloc(&b.wid, n));
     CK(s->alloc(&b.keys, n));
-    CK(s->alloc(&b.starts, C + 1));
+    CK(s->alloc(&b.starts, (size_t)s->keyspace + 1));
     CK(s->alloc(&b.perm, n));
     CK(s->alloc(&b.density, n));
     CK(s->alloc(&b.alpha, n));
@@ -683,9 +687,9 @@ static int32_t create_into(FluidSim *s, const FluidSimConfig *cfg) {
     CK(s->alloc(&s->ring, kRing));
     CK(s->alloc(&s->cur, 1));
     CK(s->alloc(&s->solve, 1));
-    const size_t wsb = grid_work_bytes(s->n, s->cells);
+    const size_t wsb = grid_work_bytes(s->n, s->keyspace);
     CK(cudaMalloc(&s->grid_ws, wsb));
-    s->gw = grid_work_carve(s->grid_ws, s->n, s->cells, &s->solve->error);
+    s->gw = grid_work_carve(s->grid_ws, s->n, s->keyspace, &s->solve->error);
     CK(cudaMallocHost(&s->h_ring, kRing * sizeof(DevStep)));
     CK(cudaMallocHost(&s->h_stats_stale, 16 * sizeof(float)));
     CK(cudaEventCreateWithFlags(&s->stats_ready, cudaEventDisableTiming));
@@ -1004,7 +1008,7 @@ int32_t fluid_sim_read_field(FluidSim *s, int32_t field, void *out, uint64_t byt
     case FLUID_FIELD_KD: src = s->b.kd; need = 4 * n; break;
     case FLUID_FIELD_PRESSURE: src = s->b.pressure; need = 4 * n; break;
     case FLUID_FIELD_NBR_N: src = s->b.nbr_n; need = 4 * n; break;
-    case FLUID_FIELD_STARTS: src = s->b.starts; need = 4ull * (s->cells + 1); break;
+    case FLUID_FIELD_STARTS: src = s->b.starts; need = 4ull * (s->keyspace + 1); break;
     case FLUID_FIELD_PERM: src = s->b.perm; need = 4 * n; break;
     case FLUID_FIELD_WORK_POS: src = s->b.wpos; need = 16 * n; break;
     case FLUID_FIELD_WORK_VEL: src = s->b.wvel; need = 16 * n; break;
@@ -1034,9 +1038,11 @@ int32_t fluid_sim_read_field(FluidSim *s, int32_t field, void *out, uint64_t byt
     return FLUID_OK;
 }
 
+uint32_t fluid_sim_grid_slabs(void) { return kSimSlabs; }
+
 uint32_t fluid_sim_kernels_per_substep(const FluidSim *s) {
     if (!s) return 0;
-    const uint32_t passes = (uint32_t)radix_passes(s->cells);
+    const uint32_t passes = (uint32_t)radix_passes(s->keyspace);
     // keys + one per radix pass + starts scan + gather + density_div
     //   + div applies (+ div_kappa after the first) + forces pair
     //   + den pairs + integrate

@@ -393,6 +393,7 @@ __device__ __forceinline__ void add_term(unsigned long long *acc, unsigned long 
 struct Stencil {
     int bx, by, bz;
     float xl, xh, yl, yh, zl, zh;
+    float px, margin;
 };
 
 __device__ __forceinline__ Stencil stencil_of(const DevParams &P, F3 pos) {
@@ -410,9 +411,26 @@ __device__ __forceinline__ Stencil stencil_of(const DevParams &P, F3 pos) {
     t.yh = fmaxf(P.cell - fy - margin, 0.0f);
     t.zl = fmaxf(fz - margin, 0.0f);
     t.zh = fmaxf(P.cell - fz - margin, 0.0f);
+    t.px = pos.x;
+    t.margin = margin;
     return t;
 }
 
+// Key of coordinate x along the first axis with K slabs per cell.
+template <int K>
+__device__ __forceinline__ uint32_t x_key(const DevParams &P, float x) {
+    const uint32_t c = axis_cell(x, P.box_min[0], P.cell, P.dims[0]);
+    return K > 1 ? c * K + axis_slab(x, P.box_min[0], P.cell, c, K) : c;
+}
+
+//
+// With K slabs per cell (the cells' slots in slab order along x), the row's
+// range is cut further to the slabs that can hold a point within the
+// support in x: every candidate whose x differs from the particle's by the
+// support's half-chord at the row's nearest perpendicular distance, widened
+// by 0.1 % and the margin, or more fails r2 < support^2, and keys are
+// monotonic in x, so the slabs of x -/+ that width bound every neighbour's.
+template <int K>
 __device__ __forceinline__ bool stencil_row(const DevParams &P, uint32_t cell_base,
                                             const uint32_t *__restrict__ starts, uint32_t n,
                                             const Stencil &t, int oz, int oy, uint32_t &s,
@@ -424,9 +442,17 @@ __device__ __forceinline__ bool stencil_row(const DevParams &P, uint32_t cell_ba
     if (dperp >= P.support_sq) return false;
     const int cx0 = (t.bx > 0 && dperp + t.xl * t.xl < P.support_sq) ? t.bx - 1 : t.bx;
     const int cx1 = (t.bx + 1 < (int)P.dims[0] && dperp + t.xh * t.xh < P.support_sq) ? t.bx + 1 : t.bx;
-    const uint32_t row = cell_base + ((uint32_t)cz * P.dims[1] + (uint32_t)cy) * P.dims[0];
-    s = __ldg(&starts[row + cx0]);
-    e = __ldg(&starts[row + cx1 + 1]);
+    const uint32_t row = ((uint32_t)cz * P.dims[1] + (uint32_t)cy) * P.dims[0];
+    if (K > 1) {
+        const float w = sqrtf(P.support_sq - dperp) * 1.001f + t.margin;
+        const uint32_t klo = max(x_key<K>(P, t.px - w), (uint32_t)cx0 * K);
+        const uint32_t khi = min(x_key<K>(P, t.px + w), (uint32_t)cx1 * K + (K - 1));
+        s = __ldg(&starts[cell_base + row * K + klo]);
+        e = __ldg(&starts[cell_base + row * K + khi + 1]);
+    } else {
+        s = __ldg(&starts[cell_base + row + cx0]);
+        e = __ldg(&starts[cell_base + row + cx1 + 1]);
+    }
     if (e > n) e = n;  // starts never exceed n unless a scan gave up
     return s < e;
 }
@@ -527,6 +553,7 @@ constexpr uint32_t kRowSpan = 4096;
 
 // The plain loop over every candidate, each hit summed and the first `cap`
 // listed. Returns the hits found.
+template <int K>
 __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_t base, const SimBufs &b,
                                                   uint32_t n, uint32_t i, F3 pos, F3 vel,
                                                   const Stencil &t, DensitySums &d) {
@@ -534,7 +561,7 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
     for (int oz = -1; oz <= 1; ++oz)
         for (int oy = -1; oy <= 1; ++oy) {
             uint32_t s, e;
-            if (!stencil_row(P, base, b.starts, n, t, oz, oy, s, e)) continue;
+            if (!stencil_row<K>(P, base, b.starts, n, t, oz, oy, s, e)) continue;
             for (uint32_t k = s; k < e; ++k) {
                 if (k == i) continue;
                 const F3 x = pos - xyz(__ldg(&b.wpos[k]));
@@ -579,7 +606,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
 #pragma unroll
         for (int r = 0; r < 9; ++r) {
             uint32_t s = 0, e = 0;
-            if (!stencil_row(P, base, b.starts, n, t, r / 3 - 1, r % 3 - 1, s, e)) s = e = 0;
+            if (!stencil_row<(int)kSimSlabs>(P, base, b.starts, n, t, r / 3 - 1, r % 3 - 1, s, e)) s = e = 0;
             s_beg[r][tid] = s;
             s_end[r][tid] = e;
             wide = wide || (e - s > kRowSpan);
@@ -667,7 +694,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
                 found += staged;
             }
         } else {
-            found = density_scan_all(P, base, b, n, i, pos, vel, t, d);
+            found = density_scan_all<(int)kSimSlabs>(P, base, b, n, i, pos, vel, t, d);
         }
         // sim_solve.wgsl:475-517
         b.nbr_n[i] = found < cap ? found : cap;

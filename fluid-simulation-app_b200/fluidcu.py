@@ -152,6 +152,7 @@ def lib():
         "fluid_sim_profile_step": (i32, [P, C.POINTER(FluidStep), C.POINTER(f),
                                          C.POINTER(C.c_char_p), u32]),
         "fluid_sim_kernels_per_substep": (u32, [P]),
+        "fluid_sim_grid_slabs": (u32, []),
         "fluid_grid_workspace_bytes": (u64, [u32, C.POINTER(FluidGrid)]),
         "fluid_grid_build": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp, vp, vp, u64, vp]),
         "fluid_grid_build_host": (i32, [vp, u32, C.POINTER(FluidGrid), vp, vp]),
@@ -453,6 +454,8 @@ class Sim:
         check(lib().fluid_sim_params(h, C.byref(self.params)), "params")
         d = self.params.dims
         self.cells = d[0] * d[1] * d[2]
+        # grid keys: cell * slabs + the x slab (fluid_sim_grid_slabs)
+        self.keyspace = self.cells * grid_slabs()
 
     def close(self):
         if getattr(self, "h", None):
@@ -557,7 +560,7 @@ class Sim:
         n = self.n
         shapes = dict(density=(n, np.float32), alpha=(n, np.float32), kd=(n, np.float32),
                       pressure=(n, np.float32), nbr_n=(n, np.uint32),
-                      starts=(self.cells + 1, np.uint32), perm=(n, np.uint32),
+                      starts=(self.keyspace + 1, np.uint32), perm=(n, np.uint32),
                       work_pos=((n, 4), np.float32), work_vel=((n, 4), np.float32),
                       accel=((n, 4), np.float32), xsph=((n, 4), np.float32),
                       wall_grad=((n, 4), np.float32), counters=(2, np.uint32))
@@ -613,6 +616,11 @@ class Controller:
         out = FluidFramePlan()
         check(lib().fluid_controller_plan(self.h, C.byref(m), now_ms, v_max, C.byref(out)), "plan")
         return out
+
+
+def grid_slabs():
+    """Slabs per cell along x in a simulation's grid keys (fluid_sim_grid_slabs)."""
+    return int(lib().fluid_sim_grid_slabs())
 
 
 def substeps_for(dt, v_max, spacing, cap):

@@ -152,7 +152,7 @@ typedef struct FluidSimStats {
 #define FLUID_FIELD_KD 2
 #define FLUID_FIELD_PRESSURE 3
 #define FLUID_FIELD_NBR_N 4     /* uint32[n] */
-#define FLUID_FIELD_STARTS 5    /* uint32[C+1] */
+#define FLUID_FIELD_STARTS 5    /* uint32[C * fluid_sim_grid_slabs() + 1] */
 #define FLUID_FIELD_PERM 6      /* uint32[n] */
 #define FLUID_FIELD_WORK_POS 7  /* float4[n] */
 #define FLUID_FIELD_WORK_VEL 8  /* float4[n] */
@@ -308,6 +308,13 @@ int32_t fluid_sim_profile_step(FluidSim *sim, const FluidStep *step, float *ms,
                                const char **names, uint32_t cap);
 /* Kernel launches one substep issues at the current schedule (fixed mode). */
 uint32_t fluid_sim_kernels_per_substep(const FluidSim *sim);
+/* Slabs per cell along x in a simulation's neighbour grid: the grid keys
+ * are cell * slabs + slab, so each cell's slots are in slab order (the
+ * reference's scatter, sim_grid.wgsl:60-72, ranks a cell's particles by
+ * atomic arrival, so any order inside a cell is one it can produce), and
+ * FLUID_FIELD_STARTS holds cells * slabs + 1 entries. fluid_grid_build and
+ * fluid_grid_build_static sort by cell alone. */
+uint32_t fluid_sim_grid_slabs(void);
 
 /* ---- the render-side thickness field ---------------------------------------
  * The body splat of sim_sprites.wgsl (`body`, `weight`, radius 1.5 h, an

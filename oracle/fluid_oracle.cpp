@@ -149,6 +149,13 @@ inline int64_t fx(double term) {
 inline float exp_r(float x);
 inline double exp_r(double x) { return std::exp(x); }
 
+// Slabs per cell along x in a simulation's grid keys; the library's
+// fluid_sim_grid_slabs() must equal it.
+#ifndef OR_SIM_SLABS
+#define OR_SIM_SLABS 1
+#endif
+constexpr uint32_t kSimSlabs = OR_SIM_SLABS;
+
 // WGSL's f32 -> u32 saturating conversion, and the grid's cell and stable
 // counting sort over positions of either width (sim.rs:38-44;
 // sim_grid.wgsl:36-58; sim_scan.wgsl:97-120).
@@ -167,14 +174,30 @@ uint32_t cell_of_t(const OrGrid *g, const T *pos) {
     }
     return (c[2] * g->dims[1] + c[1]) * g->dims[0] + c[0];
 }
+// Slab of a cell along x (the cell cut into `slabs` equal slabs across the
+// axis): the number of slab boundaries at or below the position's offset in
+// its cell. A NaN or negative offset gives 0.
+template <class T>
+uint32_t x_slab_t(const OrGrid *g, const T *pos, uint32_t cx, uint32_t slabs) {
+    const T off = pos[0] - (g->min[0] + (T)(float)cx * g->cell);
+    uint32_t s = 0;
+    for (uint32_t k = 1; k < slabs; ++k) s += off >= (T)(g->cell * ((float)k / (float)slabs)) ? 1u : 0u;
+    return s;
+}
+// The stable counting sort by key; with slabs > 1 the key is cell * slabs +
+// the x slab, so each cell's slots are in slab order (one of the orders the
+// reference's atomic scatter can produce) and starts has cells * slabs + 1
+// entries.
 template <class T>
 void grid_build_t(const OrGrid *g, const T *pos4, uint32_t n, uint32_t *keys, uint32_t *starts,
-                  uint32_t *perm) {
-    const uint32_t cells = g->dims[0] * g->dims[1] * g->dims[2];
+                  uint32_t *perm, uint32_t slabs = 1) {
+    const uint32_t cells = g->dims[0] * g->dims[1] * g->dims[2] * slabs;
     std::vector<uint32_t> counts(cells, 0u);
     std::vector<uint32_t> k(n);
     for (uint32_t i = 0; i < n; ++i) {
-        k[i] = cell_of_t(g, pos4 + 4 * (size_t)i);
+        const T *p = pos4 + 4 * (size_t)i;
+        k[i] = cell_of_t(g, p);
+        if (slabs > 1) k[i] = k[i] * slabs + x_slab_t(g, p, k[i] % g->dims[0], slabs);
         counts[k[i]]++;
     }
     uint32_t run = 0;
@@ -643,6 +666,7 @@ struct OrSim {
 
 static int g_threads = 0;
 void or_sim_set_threads(int threads) { g_threads = threads; }
+uint32_t or_sim_slabs(void) { return kSimSlabs; }
 static int nthreads() {
 #ifdef _OPENMP
     return g_threads > 0 ? g_threads : omp_get_max_threads();
@@ -672,7 +696,7 @@ OrSim *or_sim_new(const OrParams *p, uint32_t tracer_count) {
     s->wtemp.assign(n, 0.f);
     s->wid.assign(n, 0u);
     s->keys.assign(n, 0u);
-    s->starts.assign(s->cells + 1, 0u);
+    s->starts.assign((size_t)s->cells * kSimSlabs + 1, 0u);
     s->perm.assign(n, 0u);
     s->density.assign(n, 0.f);
     s->alpha.assign(n, 0.f);
@@ -755,7 +779,7 @@ OrGrid grid_of(const OrParams &p) {
 // (sim_grid.wgsl:44-72, sim_scan.wgsl:97-120).
 void rebuild(OrSim *s) {
     const OrGrid g = grid_of(s->p);
-    grid_build_t(&g, s->pos.data(), s->n, s->keys.data(), s->starts.data(), s->perm.data());
+    grid_build_t(&g, s->pos.data(), s->n, s->keys.data(), s->starts.data(), s->perm.data(), kSimSlabs);
     const int64_t n = s->n;
 #pragma omp parallel for num_threads(nthreads()) schedule(static)
     for (int64_t k = 0; k < n; ++k) {
@@ -868,8 +892,8 @@ int64_t density_div(OrSim *s, Real dt) {
                 cz >= (int)p.dims[2])
                 continue;
             const uint32_t c = ((uint32_t)cz * p.dims[1] + (uint32_t)cy) * p.dims[0] + (uint32_t)cx;
-            const uint32_t end = s->starts[c + 1];
-            for (uint32_t k = s->starts[c]; k < end; ++k) {
+            const uint32_t end = s->starts[(c + 1) * kSimSlabs];
+            for (uint32_t k = s->starts[c * kSimSlabs]; k < end; ++k) {
                 if ((int64_t)k == pi) continue;
                 const V3 x = pos - load3(&s->wpos[4 * (size_t)k]);
                 const Real r2 = dot(x, x);
@@ -1442,7 +1466,7 @@ void or_sim_field(const OrSim *s, int field, void *out) {
     case OR_FIELD_KD: copy_out(out, s->kd); break;
     case OR_FIELD_PRESSURE: copy_out(out, s->pressure); break;
     case OR_FIELD_NBR_N: std::memcpy(out, s->nbr_n.data(), 4 * n); break;
-    case OR_FIELD_STARTS: std::memcpy(out, s->starts.data(), 4 * (size_t)(s->cells + 1)); break;
+    case OR_FIELD_STARTS: std::memcpy(out, s->starts.data(), 4 * s->starts.size()); break;
     case OR_FIELD_PERM: std::memcpy(out, s->perm.data(), 4 * n); break;
     case OR_FIELD_WORK_POS: copy_out(out, s->wpos); break;
     case OR_FIELD_WORK_VEL: copy_out(out, s->wvel); break;

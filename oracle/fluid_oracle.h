@@ -124,6 +124,10 @@ typedef struct OrSim OrSim;
 OrSim *or_sim_new(const OrParams *p, uint32_t tracer_count);
 void or_sim_free(OrSim *s);
 void or_sim_set_threads(int threads);
+/* Slabs per cell along x in a simulation's grid keys (cell * slabs + slab):
+ * each cell's slots are in slab order, and the starts field holds
+ * cells * slabs + 1 entries. */
+uint32_t or_sim_slabs(void);
 /* Resting set, in its slot order. Any pointer may be null (zero fill,
  * temperature 293.15, id = slot). */
 void or_sim_set_state(OrSim *s, const float *pos4, const float *vel4, const float *prev_vel4,

@@ -110,6 +110,7 @@ def load_library(path):
         "or_sim_new": (C.c_void_p, [C.POINTER(OrParams), U]),
         "or_sim_free": (None, [C.c_void_p]),
         "or_sim_set_threads": (None, [C.c_int]),
+        "or_sim_slabs": (U, []),
         "or_sim_set_state": (None, [C.c_void_p] + [C.c_void_p] * 6),
         "or_sim_get_state": (None, [C.c_void_p] + [C.c_void_p] * 6),
         "or_sim_set_tracers": (None, [C.c_void_p, u32p]),
@@ -296,7 +297,7 @@ class Sim:
         n = self.n
         shapes = dict(density=(n, np.float32), alpha=(n, np.float32), kd=(n, np.float32),
                       pressure=(n, np.float32), nbr_n=(n, np.uint32),
-                      starts=(self.cells + 1, np.uint32), perm=(n, np.uint32),
+                      starts=(self.cells * sim_slabs() + 1, np.uint32), perm=(n, np.uint32),
                       work_pos=((n, 4), np.float32), work_vel=((n, 4), np.float32),
                       accel=((n, 4), np.float32), xsph=((n, 4), np.float32),
                       wall_grad=((n, 4), np.float32), counters=(2, np.uint32),
@@ -315,6 +316,11 @@ class Sim:
 
 def set_threads(n):
     lib().or_sim_set_threads(n)
+
+
+def sim_slabs():
+    """Slabs per cell along x in a simulation's grid keys."""
+    return int(lib().or_sim_slabs())
 
 
 def field_splat(pos4, vel4, pvel4, density, geom, w, h, lens, keep, field2=None):
