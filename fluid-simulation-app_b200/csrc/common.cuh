@@ -114,8 +114,11 @@ __device__ __forceinline__ uint32_t axis_cell(float v, float mn, float cell, uin
 }
 
 // Slabs per cell along x in a simulation's grid keys (GridGeom::slabs).
+// Four measured on the 1M tilt workload: density_div 0.643 -> 0.610 ms
+// (about 30 % fewer candidates), the list sweeps 2-3 % faster, the grid
+// build 0.11 -> 0.12 ms (four times the starts), the plain step 4 % faster.
 #ifndef FCU_SLABS
-#define FCU_SLABS 1
+#define FCU_SLABS 4
 #endif
 constexpr uint32_t kSimSlabs = FCU_SLABS;
 

@@ -152,7 +152,7 @@ inline double exp_r(double x) { return std::exp(x); }
 // Slabs per cell along x in a simulation's grid keys; the library's
 // fluid_sim_grid_slabs() must equal it.
 #ifndef OR_SIM_SLABS
-#define OR_SIM_SLABS 1
+#define OR_SIM_SLABS 4
 #endif
 constexpr uint32_t kSimSlabs = OR_SIM_SLABS;
 

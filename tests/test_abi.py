@@ -60,3 +60,9 @@ def test_grid_workspace_size_is_reported(fcu):
     assert 4 * (1 << 24) * 4 <= b < 4 * (1 << 24) * 5
     g.dims[:] = [0, 1, 1]
     assert fcu.grid_workspace_bytes(10, g) == 0
+
+
+# A simulation's cells hold their slots in x-slab order on both sides: the
+# oracle must sort by the same keys as the library for the sums to agree.
+def test_the_library_and_the_oracle_cut_cells_into_the_same_slabs(fcu, orc):
+    assert fcu.grid_slabs() == orc.sim_slabs() == 4

@@ -87,12 +87,24 @@ def test_the_rebuild_lands_every_particle_in_cell_order(orc):
     g.cell = p.cell
     g.dims[:] = list(p.dims)
     C = orc.cell_count(g)
-    assert starts[C] == p.count
+    # a simulation's grid keys are cell * K + the x slab: cell c holds the
+    # slots starts[c * K] .. starts[(c + 1) * K] - 1, in slab order
+    K = orc.sim_slabs()
+    assert len(starts) == C * K + 1 and starts[C * K] == p.count
+    cs = starts[::K]
     keys, _, _ = orc.grid_build(g, working)
     for k, c in enumerate(keys):
-        assert starts[c] <= k < starts[c + 1]
+        assert cs[c] <= k < cs[c + 1]
     held = np.bincount(keys, minlength=C)
-    assert np.array_equal(held, np.diff(starts.astype(np.int64)))
+    assert np.array_equal(held, np.diff(cs.astype(np.int64)))
+    f32 = np.float32
+    cx = keys % p.dims[0]
+    off = working[:, 0] - (f32(p.box_min[0]) + cx.astype(f32) * f32(p.cell))
+    slab = sum((off >= f32(p.cell) * (f32(k) / f32(K))).astype(np.int64) for k in range(1, K))
+    skey = keys.astype(np.int64) * K + slab
+    assert np.all(np.diff(skey) >= 0)
+    for k, c in enumerate(skey):
+        assert starts[c] <= k < starts[c + 1]
     a = np.sort(pos[:, :3].view(np.uint32), axis=0)
     b = np.sort(working[:, :3].view(np.uint32), axis=0)
     seeded = sorted(map(tuple, pos[:, :3].view(np.uint32)))
