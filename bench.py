@@ -71,9 +71,9 @@ ALGO_BYTES = {"grid": 20.0, "gather": 116.0, "density_div": 44.0, "div_kappa": 2
 # particles, on the state after the benchmark's 25 frames
 # (dram__bytes_read.sum + dram__bytes_write.sum), not measured by this
 # script; a kernel change calls for a new capture.
-NCU_TRAFFIC_PER_PARTICLE = {"density_div": (100.93e6 + 329.28e6) / 1048576,
-                            "forces_eval": (415.34e6 + 37.60e6) / 1048576,
-                            "den_kappa": (423.84e6 + 16.27e6) / 1048576}
+NCU_TRAFFIC_PER_PARTICLE = {"density_div": (106.80e6 + 318.62e6) / 1048576,
+                            "forces_eval": (410.57e6 + 38.01e6) / 1048576,
+                            "den_kappa": (406.19e6 + 15.34e6) / 1048576}
 
 
 def workload_config(w, n):

@@ -33,8 +33,15 @@
 // scaled for other block sizes; a batch too: its instance measured 3 %
 // faster held to it) and the one box's kappa sweeps are compiled for (0:
 // none), and density_div's hits staged per round.
+// density_div at 8 blocks (64 registers, 24 bytes spilled) measured 0.590
+// against 0.608 ms at 7 (72 registers) and 0.624 at 6 on the 1M workload
+// with four x slabs per cell.
 #ifndef FCU_MINB_DD
-#define FCU_MINB_DD 7
+#define FCU_MINB_DD 8
+#endif
+// The batch's instance (box lookups) spills 58 bytes at 8 blocks.
+#ifndef FCU_MINB_DD_BATCH
+#define FCU_MINB_DD_BATCH 7
 #endif
 #ifndef FCU_MINB_KAPPA
 #define FCU_MINB_KAPPA 0
@@ -576,7 +583,7 @@ __device__ __forceinline__ uint32_t density_scan_all(const DevParams &P, uint32_
 }
 
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB_DD * 128 / TPB)
+__global__ void __launch_bounds__(TPB, (kB ? FCU_MINB_DD_BATCH : FCU_MINB_DD) * 128 / TPB)
     k_density_div(const __grid_constant__ Geo g, SimBufs b, int slot) {
     __shared__ uint16_t s_hit[kStage + FCU_DD_CHUNK - 1][TPB];
     __shared__ uint32_t s_beg[9][TPB];
