@@ -64,6 +64,13 @@ constexpr int kBatchKappaThreads = 768;
 #ifndef FCU_MINB
 #define FCU_MINB 0
 #endif
+// One box's forces_eval (plain and with the divergence prediction) at 8
+// blocks of 128 threads per SM (64 registers; the fused one spills 24
+// bytes): frames 1.1 % shorter on the 1M workload than at its 72 / 76
+// registers (7 / 6 blocks). Scaled for other block sizes like density_div.
+#ifndef FCU_MINB_FORCES
+#define FCU_MINB_FORCES 8
+#endif
 
 namespace fcu {
 
@@ -910,7 +917,7 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
 }
 
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
+__global__ void __launch_bounds__(TPB, kB ? FCU_MINB : FCU_MINB_FORCES * 128 / TPB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
 #if FCU_SORTED_FORCES
     const uint32_t i = slot_by_count<TPB>(b.nbr_n, g.n);
 #else
@@ -919,7 +926,7 @@ __global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_plain(Geo g, SimBufs b
     forces_eval_body<kB, false>(g, b, i, i < g.n, slot, gate);
 }
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, FCU_MINB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
+__global__ void __launch_bounds__(TPB, kB ? FCU_MINB : FCU_MINB_FORCES * 128 / TPB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
 #if FCU_SORTED_FORCES
     const uint32_t i = slot_by_count<TPB>(b.nbr_n, g.n);
 #else
