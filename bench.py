@@ -76,6 +76,17 @@ NCU_TRAFFIC_PER_PARTICLE = {"density_div": (106.80e6 + 318.62e6) / 1048576,
                             "den_kappa": (406.19e6 + 15.34e6) / 1048576}
 
 
+# What holds each leading kernel back, from the same ncu capture: none of
+# them is DRAM-bound, so their fraction of the HBM roofline stays low.
+NCU_LIMITER = {
+    "density_div": "SM issue and L1 (ncu: 65 % SM throughput, 68 % issue active, 65 % L1 "
+                   "wavefronts, 43 % warps active; ~194 candidate tests and ~33 hits a particle)",
+    "forces_eval": "SM issue (ncu: 72 % SM throughput, 76 % issue active; ten IEEE divisions "
+                   "and a square root per pair)",
+    "den_kappa": "L1 data pipe (ncu: 80 % L1 wavefronts; neighbour records gathered through L1)",
+}
+
+
 def workload_config(w, n):
     """The workload both arms run, as the JSON line's `config`."""
     return {"workload": WORKLOAD, "particles": n, "lattice": "x".join(str(v) for v in w["lattice"]),
@@ -363,6 +374,7 @@ def cuda_arm(args):
                                            "not measured in this run",
                          "peak_source": f"{peak_kind} MEASURED_PEAKS.json hbm_gbs" if peak_kind == "measured" else "fallback 6.65 TB/s",
                          "algorithmic": f"own records, list-free ({ALGO_BYTES[dom]:.0f} B per particle for {dom})",
+                         "limiter": NCU_LIMITER.get(dom),
                          "mean_neighbours": mean_nbrs,
                          "achieved_with_list": (ALGO_BYTES[dom] + list_bytes) * n / (avg_ms / 1000.0) / 1e9,
                          "frac_with_list": (ALGO_BYTES[dom] + list_bytes) * n / (avg_ms / 1000.0) / 1e9 / peak,
