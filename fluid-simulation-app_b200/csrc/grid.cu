@@ -360,6 +360,13 @@ static_assert(kRadix == kSortThreads, "one thread per digit");
 #ifndef FCU_SORT_MATCH
 #define FCU_SORT_MATCH 0
 #endif
+// FCU_VAL_PREFETCH > 0: a digit pass asks L1 for the values of every
+// FCU_VAL_PREFETCH-th round of its tile while it ranks the keys. Measured:
+// grid_16m 0.683 -> 0.648 ms a build at 1 (0.676 at 4); the 1M workload's
+// grid 0.1153 -> 0.1147 ms.
+#ifndef FCU_VAL_PREFETCH
+#define FCU_VAL_PREFETCH 1
+#endif
 // Earlier tiles' status words a digit's look-back loads at once. Measured:
 // the 1M workload's grid 0.1215 ms at 1, 0.1158 at 4, 0.1157 at 8 (16 bytes
 // spilled), 0.1203 at 16; grid_16m 0.70 / 0.68 / 0.69 / 0.74 ms a build.
@@ -405,6 +412,17 @@ __global__ void __launch_bounds__(kSortThreads, FCU_SORT_MINB) k_radix_pass(
             key[r] = i < n ? __ldg(&keys_in[i]) : 0u;
         }
     }
+#if FCU_VAL_PREFETCH
+    // the values are read only after the ranking and the look-back: ask L1
+    // for them now (no registers held) so that read finds them there
+    if (vals_in) {
+#pragma unroll
+        for (int r = 0; r < kSortItems; r += FCU_VAL_PREFETCH) {
+            const uint32_t i = wbase + r * 32 + lane;
+            if (full || i < n) asm volatile("prefetch.global.L1 [%0];" ::"l"(vals_in + i));
+        }
+    }
+#endif
     // every round's digit peers first (ballots and registers only), then the
     // rounds in order: the leader of each group of peers adds the group to
     // the warp's count of its digit and hands the old count to the group
