@@ -71,6 +71,11 @@ constexpr int kBatchKappaThreads = 768;
 #ifndef FCU_MINB_FORCES
 #define FCU_MINB_FORCES 8
 #endif
+// The batch's forces_eval at 7 blocks of 128 per SM (scaled likewise):
+// batched_256 8.88 against 9.05 ms a substep with no floor, 9.12 at 8.
+#ifndef FCU_MINB_FORCES_BATCH
+#define FCU_MINB_FORCES_BATCH 7
+#endif
 
 namespace fcu {
 
@@ -917,7 +922,7 @@ __device__ __forceinline__ void forces_eval_body(const Geo &g, const SimBufs &b,
 }
 
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, kB ? FCU_MINB : FCU_MINB_FORCES * 128 / TPB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
+__global__ void __launch_bounds__(TPB, kB ? FCU_MINB_FORCES_BATCH * 128 / TPB : FCU_MINB_FORCES * 128 / TPB) k_forces_plain(Geo g, SimBufs b, int slot, int gate) {
 #if FCU_SORTED_FORCES
     const uint32_t i = slot_by_count<TPB>(b.nbr_n, g.n);
 #else
@@ -926,7 +931,7 @@ __global__ void __launch_bounds__(TPB, kB ? FCU_MINB : FCU_MINB_FORCES * 128 / T
     forces_eval_body<kB, false>(g, b, i, i < g.n, slot, gate);
 }
 template <bool kB, int TPB>
-__global__ void __launch_bounds__(TPB, kB ? FCU_MINB : FCU_MINB_FORCES * 128 / TPB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
+__global__ void __launch_bounds__(TPB, kB ? FCU_MINB_FORCES_BATCH * 128 / TPB : FCU_MINB_FORCES * 128 / TPB) k_forces_fused(Geo g, SimBufs b, int slot, int gate) {
 #if FCU_SORTED_FORCES
     const uint32_t i = slot_by_count<TPB>(b.nbr_n, g.n);
 #else
