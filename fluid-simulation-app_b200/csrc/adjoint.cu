@@ -64,6 +64,13 @@ namespace {
 
 constexpr int kAdjThreads = 128;
 constexpr uint32_t kModelCap = 128;  // neighbours a particle may have in the model
+// The model's grid keys are cell * kAdjSlabs + the x slab, as a simulation's:
+// each cell's particles in slab order, so the density sweep can skip the
+// stencil cells and x slabs beyond the support (ADJ_CULL).
+constexpr uint32_t kAdjSlabs = kSimSlabs;
+#ifndef ADJ_CULL
+#define ADJ_CULL 1
+#endif
 
 // ---- small vector and dual types --------------------------------------------
 template <class T>
@@ -431,14 +438,46 @@ __global__ void __launch_bounds__(kAdjThreads) k_m_density(MP<T> p, uint32_t n, 
     T w_sum = p.sigma, near = T(0), gsq = T(0);
     V3<T> gsum = zero3<T>();
     uint32_t cnt = 0;
+#if ADJ_CULL
+    // Stencil cells and x slabs beyond the support skipped, as in the
+    // simulation's density sweep: on the float position the grid was built
+    // from, the distances to the own cell's faces shrunk by a margin far
+    // above both its rounding and the float / T difference of positions.
+    const float cellf = p.cell, sup2f = (float)p.sup2;
+    const float margin = 1e-3f * cellf + 1e-6f * (fabsf(pf.x) + fabsf(pf.y) + fabsf(pf.z));
+    const float fx = pf.x - (p.box_min[0] + (float)bx * cellf);
+    const float fy = pf.y - (p.box_min[1] + (float)by * cellf);
+    const float fz = pf.z - (p.box_min[2] + (float)bz * cellf);
+    const float xl = fmaxf(fx - margin, 0.0f), xh = fmaxf(cellf - fx - margin, 0.0f);
+    const float yl = fmaxf(fy - margin, 0.0f), yh = fmaxf(cellf - fy - margin, 0.0f);
+    const float zl = fmaxf(fz - margin, 0.0f), zh = fmaxf(cellf - fz - margin, 0.0f);
+#endif
     for (int oz = -1; oz <= 1; ++oz)
         for (int oy = -1; oy <= 1; ++oy) {
             const int cz = bz + oz, cy = by + oy;
             if (cz < 0 || cz >= (int)p.dims[2] || cy < 0 || cy >= (int)p.dims[1]) continue;
+            const uint32_t row = ((uint32_t)cz * p.dims[1] + (uint32_t)cy) * p.dims[0];
+#if ADJ_CULL
+            const float dperp = (oz < 0 ? zl * zl : (oz > 0 ? zh * zh : 0.0f)) +
+                                (oy < 0 ? yl * yl : (oy > 0 ? yh * yh : 0.0f));
+            if (dperp >= sup2f) continue;
+            const int cx0 = (bx > 0 && dperp + xl * xl < sup2f) ? bx - 1 : bx;
+            const int cx1 = (bx + 1 < (int)p.dims[0] && dperp + xh * xh < sup2f) ? bx + 1 : bx;
+            const float w = sqrtf(sup2f - dperp) * 1.001f + margin;
+            const float xa = pf.x - w, xb = pf.x + w;
+            const uint32_t ca = axis_cell(xa, p.box_min[0], cellf, p.dims[0]);
+            const uint32_t cb = axis_cell(xb, p.box_min[0], cellf, p.dims[0]);
+            const uint32_t klo = max(ca * kAdjSlabs + axis_slab(xa, p.box_min[0], cellf, ca, kAdjSlabs),
+                                     (uint32_t)cx0 * kAdjSlabs);
+            const uint32_t khi = min(cb * kAdjSlabs + axis_slab(xb, p.box_min[0], cellf, cb, kAdjSlabs),
+                                     (uint32_t)cx1 * kAdjSlabs + (kAdjSlabs - 1));
+            uint32_t s = starts[row * kAdjSlabs + klo], e = starts[row * kAdjSlabs + khi + 1];
+            if (s > e) s = e;
+#else
             const int cx0 = bx > 0 ? bx - 1 : bx;
             const int cx1 = bx + 1 < (int)p.dims[0] ? bx + 1 : bx;
-            const uint32_t row = ((uint32_t)cz * p.dims[1] + (uint32_t)cy) * p.dims[0];
-            uint32_t s = starts[row + cx0], e = starts[row + cx1 + 1];
+            uint32_t s = starts[(row + cx0) * kAdjSlabs], e = starts[(row + cx1 + 1) * kAdjSlabs];
+#endif
             if (e > n) e = n;
             // candidates four at a time: their positions load together
             for (uint32_t k0 = s; k0 < e; k0 += 4) {
@@ -1444,8 +1483,8 @@ struct AdjImpl : AdjBase {
         dt = T(dts);
         vclamp = T(vclamp_);
         const uint64_t c64 = (uint64_t)P.dims[0] * P.dims[1] * P.dims[2];
-        if (c64 >= 0xffffffffull) return report_error(FLUID_ERR_ARG, "adjoint: grid has too many cells");
-        cells = (uint32_t)c64;
+        if (c64 * kAdjSlabs >= 0xffffffffull) return report_error(FLUID_ERR_ARG, "adjoint: grid has too many cells");
+        cells = (uint32_t)(c64 * kAdjSlabs);  // grid keys: cell * slabs + x slab
         AK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         const size_t N = n;
         AK(alloc(&pos4, N));
@@ -1530,6 +1569,7 @@ struct AdjImpl : AdjBase {
             g.dims[a] = P.dims[a];
         }
         g.cell = P.cell;
+        g.slabs = kAdjSlabs;
         AK(cudaMemsetAsync(gw.err, 0, 4, stream));
         AK(grid_build_enqueue(stream, pos4, n, g, keys, starts, perm, gw, nullptr, nullptr, nullptr, 1));
         return FLUID_OK;
